@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""PairHMM GCUPS on B200: the batched FP32-scaled forward against the reference CPU path.
+
+Workload (configs[1] shape): 10,000 synthetic regions, 2-16 haplotypes of
+100-1,000 bp, lognormal(median 60) reads of 100-250 bp, gap-open Q45 /
+gap-continuation Q10 (vardepth_b200/synthetic.py, seed 1).  A step scores every
+read against every haplotype of its region.
+
+  value    GCUPS of the device-resident plan: the captured CUDA graph of the three
+           kernel tiers (FP32 wavefront, FP64 rescue, FP64 32-row strips) on inputs
+           already in HBM, timed with CUDA events on the engine stream, max over ranks.
+  e2e      GCUPS through the C-ABI call vd_forward with pinned host buffers: work-list
+           build, host->device copies, kernels and the device->host copy of the
+           results inside the timed region.
+  roofline FP32-pipe roofline of the primary kernel: 12 algorithmic flops per cell
+           (wide.cpp:19-21) / its event-timed duration, against the FP32 FMA peak
+           measured on the same device by vd_measure_fp32_peak.
+  cpu_baseline  the reference's own C++ (oracle/_ref/libwide.so, compiled from
+           caller/native/caller/wide.cpp) read_haplotype_batch_mode on every host
+           core, on a deterministic region subsample of the same workload.
+
+--impl reference times only that CPU implementation (rank 0), one subsample pass
+per step.  Multi-GPU: one process per GPU under torchrun, each rank scores its
+own copy of the workload (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PairHMM GCUPS on 1 B200, batched vs plain, at ≤1e-4 log10L err vs FP64"
+FLOPS_PER_CELL = 12          # M: 2 mul + 2 add + 1 emission; I: 3 mul + 1 add; D: 2 mul + 1 add (wide.cpp:19-21)
+NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--regions", type=int, default=10_000)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---- CPU reference (oracle/_ref, the reference's own wide.cpp) -----------------------
+
+def _cpu_jobs(w, regions):
+    """Pre-encoded ctypes arguments of read_haplotype_batch_mode, one job per read."""
+    import ctypes
+    jobs = []
+    cells = 0
+    for g in regions:
+        h0, h1 = w.region_hap_off[g], w.region_hap_off[g + 1]
+        haps = [bytes(w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]]) for h in range(h0, h1)]
+        hp = (ctypes.c_char_p * len(haps))(*haps)
+        hl = (ctypes.c_int * len(haps))(*map(len, haps))
+        msum = sum(map(len, haps))
+        for r in range(w.region_read_off[g], w.region_read_off[g + 1]):
+            a, b = w.read_off[r], w.read_off[r + 1]
+            seq = bytes(w.read_bases[a:b])
+            q = (ctypes.c_ubyte * (b - a)).from_buffer_copy(w.read_quals[a:b].tobytes())
+            out = np.empty(len(haps))
+            jobs.append((seq, q, b - a, hp, hl, len(haps), out, haps))
+            cells += (b - a) * msum
+    return jobs, cells
+
+
+def _run_cpu(jobs, gap, ext, threads):
+    import ctypes
+    from oracle import oracle as O
+    lib = O.ref_lib("wide")
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def one(j):
+        seq, q, n, hp, hl, k, out, _ = j
+        lib.read_haplotype_batch_mode(seq, q, n, hp, hl, k, gap, ext, out.ctypes.data_as(dp), 0)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        list(pool.map(one, jobs, chunksize=4))
+    return time.perf_counter() - t0
+
+
+def cpu_reference(w, seconds, repeats=1, per_step=False):
+    """Rate of the reference CPU path on a deterministic region subsample sized to ~`seconds`."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        O.build()
+    threads = O.host_cores()
+    order = np.random.default_rng(12345).permutation(w.n_regions)
+    # calibrate on a small prefix of the order
+    k = 1
+    while True:
+        jobs, cells = _cpu_jobs(w, order[:k])
+        if cells >= 2e8 or k >= len(order):
+            break
+        k = min(len(order), k * 2)
+    t = _run_cpu(jobs, w.gap, w.ext, threads)
+    rate = cells / t
+    need = rate * seconds
+    k2 = max(k, int(np.ceil(0.01 * w.n_regions)))
+    cum = 0
+    sizes = np.array([(w.read_off[w.region_read_off[g + 1]] - w.read_off[w.region_read_off[g]]) *
+                      (w.hap_off[w.region_hap_off[g + 1]] - w.hap_off[w.region_hap_off[g]]) for g in order])
+    cum = np.cumsum(sizes)
+    k2 = max(k2, int(np.searchsorted(cum, need)) + 1)
+    k2 = min(k2, len(order))
+    jobs, cells = _cpu_jobs(w, order[:k2])
+    times = [_run_cpu(jobs, w.gap, w.ext, threads) for _ in range(repeats)]
+    import platform
+    model = ""
+    try:
+        model = next(l.split(":", 1)[1].strip() for l in open("/proc/cpuinfo") if l.startswith("model name"))
+    except (OSError, StopIteration):
+        model = platform.processor()
+    sample = (f"{k2} of {w.n_regions} regions (seeded order), {cells:.3e} cells, "
+              f"read_haplotype_batch_mode (AVX-512 8-lane) on {threads} threads, {model}")
+    return dict(cells=cells, times=times, threads=threads, sample=sample, jobs=jobs)
+
+
+# ---- clocks ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i] == "Active"})
+        pw = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows), "power_w_median": statistics.median(pw) if pw else None}
+
+
+# ---- main -------------------------------------------------------------------------------
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from vardepth_b200 import synthetic
+    w = synthetic.config1(n_regions=args.regions)
+    per_step = max(2.0, args.cpu_seconds)
+    res = cpu_reference(w, per_step, repeats=0)
+    jobs, cells, threads = res["jobs"], res["cells"], res["threads"]
+    for _ in range(args.warmup):
+        _run_cpu(jobs, w.gap, w.ext, threads)
+    times = [_run_cpu(jobs, w.gap, w.ext, threads) for _ in range(args.steps)]
+    total = sum(times)
+    value = cells * args.steps / total / 1e9
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "GCUPS", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "configs[1]: 10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of "
+                                   "100-250 bp, gap-open Q45, gap-cont Q10", "regions": args.regions,
+                       "pairs": w.pairs(), "cells": w.cells(), "step": "one pass over the CPU sample"},
+            "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                             "sample": res["sample"]},
+            "e2e": {"value": round(value, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+
+    from vardepth_b200 import native, synthetic
+    w = synthetic.config1(n_regions=args.regions)
+    cells, pairs = w.cells(), w.pairs()
+
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8).pin_memory()
+        v = t.numpy().view(a.dtype)
+        v[:] = a.reshape(-1)
+        return t, v
+
+    keep = []
+    arrays = {}
+    for name in ("read_bases", "read_quals", "read_off", "hap_bases", "hap_off", "region_read_off", "region_hap_off"):
+        t, v = pinned(getattr(w, name))
+        keep.append(t)
+        arrays[name] = v
+    packed = native.Packed(arrays["read_bases"], arrays["read_quals"], arrays["read_off"], arrays["hap_bases"],
+                           arrays["hap_off"], region_read_off=arrays["region_read_off"],
+                           region_hap_off=arrays["region_hap_off"])
+    engine = native.Engine(local, 65536)
+    info = engine.info()
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    peak = __import__("ctypes").c_double()
+    native.check(native.library().vd_measure_fp32_peak(local, __import__("ctypes").byref(peak)), "fp32 peak")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident batches (value) ----
+    plan = engine.plan(packed, params)
+    for _ in range(max(3, args.warmup)):
+        plan.run()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        uuid = None
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    kernel_ms = primary_ms = 0.0
+    rescued = 0
+    launches = 0
+    for _ in range(args.steps):
+        st = plan.run()
+        kernel_ms += st.kernel_ms
+        primary_ms += st.primary_ms
+        rescued = st.rescued_fp64 + st.rescued_robust
+        launches += st.kernel_launches
+    torch.cuda.synchronize()
+    barrier()
+    sampler.stop()
+    kernel_ms = allmax(kernel_ms)
+    step_ms = kernel_ms / args.steps
+    value = world * cells / (step_ms / 1e3) / 1e9
+    got = plan.fetch()
+    plan.close()
+
+    # ---- parity spot check on a region subsample (oracle, CPU) ----
+    parity = None
+    if rank == 0:
+        from oracle import oracle as O
+        sub = np.random.default_rng(7).choice(w.n_regions, size=min(24, w.n_regions), replace=False)
+        offs = np.concatenate([[0], np.cumsum(np.diff(w.region_read_off) * np.diff(w.region_hap_off))])
+        idx = np.concatenate([np.arange(offs[g], offs[g + 1]) for g in sub])
+        sw = w.subset(sub)
+        pr, ph = sw.explicit_pairs()
+        want = O.forward_pairs(sw.read_bases, sw.read_quals, sw.read_off, sw.hap_bases, sw.hap_off, pr, ph, w.gap,
+                               w.ext, threads=0)
+        err = np.abs(got[idx] - want) / np.log(10.0)
+        parity = {"pairs_checked": int(len(idx)), "max_abs_dlog10": float(err.max()),
+                  "p99_abs_dlog10": float(np.quantile(err, 0.99)), "oracle": "FP64 restatement (oracle/)"}
+
+    # ---- end to end through vd_forward with pinned host buffers (e2e) ----
+    e2e = None
+    if not args.no_e2e:
+        out_t = torch.empty(pairs * 8, dtype=torch.uint8).pin_memory()
+        out = out_t.numpy().view(np.float64)
+        for _ in range(max(1, args.warmup)):
+            engine.forward(packed, params, out)
+        barrier()
+        torch.cuda.synchronize()
+        wall = 0.0
+        st = None
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            _, st = engine.forward(packed, params, out)
+            wall += time.perf_counter() - t0
+        torch.cuda.synchronize()
+        barrier()
+        wall = allmax(wall)
+        e2e = {"value": round(world * cells / (wall / args.steps) / 1e9, 3), "unit": "GCUPS",
+               "h2d_bytes_per_step": int(st.h2d_bytes), "d2h_bytes_per_step": int(st.d2h_bytes),
+               "ms_per_step": round(1e3 * wall / args.steps, 3), "host_ms_per_step": round(st.host_ms, 3),
+               "api": "vd_forward (C ABI), pinned host inputs and outputs"}
+        if np.max(np.abs(out - got)) != 0.0:
+            raise SystemExit("vd_forward and the resident plan disagree")
+
+    # ---- CPU baseline (reference code, rank 0 at N=1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        res = cpu_reference(w, args.cpu_seconds)
+        cpu = {"value": round(res["cells"] / res["times"][0] / 1e9, 4), "unit": "GCUPS", "cores": res["threads"],
+               "kind": "reference", "sample": res["sample"]}
+
+    primary_ms = allmax(primary_ms) / args.steps
+    achieved = cells * FLOPS_PER_CELL / (primary_ms / 1e3) / 1e12
+    traffic = None
+    tf = ROOT / "profiles" / "pairhmm_f32_traffic.json"
+    if tf.exists():
+        try:
+            t = json.loads(tf.read_text())
+            traffic = t.get("bytes_per_launch_full_config1")
+        except (OSError, ValueError):
+            traffic = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": round(step_ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": "configs[1]: 10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of "
+                                   "100-250 bp, gap-open Q45, gap-cont Q10",
+                       "regions": args.regions, "pairs": pairs, "cells": cells, "seed": 1,
+                       "inputs_bytes": w.input_bytes(), "l2": "inputs (%.2f GB) exceed the 126 MB L2; "
+                       "the recurrence state lives in registers" % (w.input_bytes() / 1e9),
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "precision": "FP32 scaled, FP64 rescue", "gpu": info["gpu"]},
+            "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak.value, 3),
+                         "unit": "TFLOP/s", "frac": round(achieved / peak.value, 4), "traffic": traffic,
+                         "flops_per_cell": FLOPS_PER_CELL, "kernel": "pairhmm_kernel<float> (primary tier)",
+                         "primary_ms": round(primary_ms, 3),
+                         "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
+                         "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "rescued_pairs": int(rescued), "parity": parity, "clocks": sampler.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    engine.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

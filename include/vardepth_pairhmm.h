@@ -1,0 +1,167 @@
+/*
+ * vardepth_pairhmm.h — C ABI of the B200 (sm_100a) PairHMM read x haplotype
+ * likelihood stage.  Link against libvardepth_pairhmm.so.
+ *
+ * Results are natural-log likelihoods (float64), like every reference entry
+ * point; an empty read or haplotype gives -inf.  Status codes follow the
+ * reference's C ABI (caller/native/caller/batch_hmm.cpp:217-219,
+ * trie_vector.cpp:284-286): 0 = OK, 1 = bad arguments; codes >= 2 are device
+ * errors this library adds.  vd_last_error() describes the last failure of
+ * the calling thread.  All inputs are caller-owned host memory; nothing is
+ * retained after a call returns (plans excepted, see below).
+ */
+#ifndef VARDEPTH_PAIRHMM_H
+#define VARDEPTH_PAIRHMM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  VD_OK = 0,
+  VD_EINVAL = 1,   /* bad arguments (same meaning as the reference's return 1) */
+  VD_ECUDA = 2,    /* CUDA runtime error */
+  VD_ENODEV = 3,   /* no usable CUDA device */
+  VD_ENOMEM = 4,   /* device or host allocation failed, or a pair exceeds the budget */
+  VD_EOVERFLOW = 5 /* a rescue list overflowed (internal capacity error) */
+};
+
+enum {
+  VD_PRECISION_MIXED = 0,   /* FP32 scaled wavefront, FP64 rescue of underflowing pairs */
+  VD_PRECISION_FLOAT64 = 1  /* every pair in the FP64 wavefront */
+};
+
+/* Model parameters of one call. */
+typedef struct vd_params {
+  double gap;       /* gap-open probability g (reference production value 0.001) */
+  double ext;       /* gap-continuation probability x (reference value 0.1) */
+  int anchored;     /* 0: semiglobal (wide.cpp:9-33), 1: anchored/global (anchored.cpp:5-25) */
+  int precision;    /* VD_PRECISION_* */
+  const double *quality_offsets; /* NULL, or 4 Phred offsets added per quality bin
+                                    (bins: q<15, q<25, q<35, q>=35); no counterpart in
+                                    the reference, NULL reproduces it exactly */
+  int reserved[4];  /* must be zero */
+} vd_params;
+
+/* A batch of reads and haplotypes in packed buffers.  Read r occupies
+ * read_bases/read_quals[read_off[r] .. read_off[r+1]); haplotype h occupies
+ * hap_bases[hap_off[h] .. hap_off[h+1]).  Bases are the reference's bytes
+ * (ASCII ACGTN, compared as plain bytes); qualities are Phred bytes 0..255.
+ *
+ * The pairs to score are given either
+ *  - as regions (pair_read == NULL): region g scores every read in
+ *    [region_read_off[g], region_read_off[g+1]) against every haplotype in
+ *    [region_hap_off[g], region_hap_off[g+1]); the output holds the regions in
+ *    order, each a reads x haplotypes row-major block (trie_vector.cpp:284-292
+ *    layout, one block per region); or
+ *  - as explicit pairs (pair_read != NULL): out[p] scores read pair_read[p]
+ *    against haplotype pair_hap[p] (batch_hmm.cpp:217 semantics). */
+typedef struct vd_batch {
+  const unsigned char *read_bases;
+  const unsigned char *read_quals;
+  const int64_t *read_off;   /* n_reads + 1 */
+  int64_t n_reads;
+  const unsigned char *hap_bases;
+  const int64_t *hap_off;    /* n_haps + 1 */
+  int64_t n_haps;
+  const int64_t *region_read_off; /* n_regions + 1 (region form) */
+  const int64_t *region_hap_off;  /* n_regions + 1 (region form) */
+  int64_t n_regions;
+  const int32_t *pair_read;  /* n_pairs (pair form) */
+  const int32_t *pair_hap;   /* n_pairs (pair form) */
+  int64_t n_pairs;
+} vd_batch;
+
+/* Telemetry of one call (the reference's CudaPairHMM.last, accelerator.py:155-158). */
+typedef struct vd_stats {
+  int64_t pairs;            /* output slots */
+  int64_t dp_cells;         /* sum of n*m over non-empty pairs */
+  int64_t work_items;       /* warp work items of the primary tier */
+  int64_t batches;          /* memory-budget chunks */
+  int64_t rescued_fp64;     /* pairs recomputed in the FP64 wavefront */
+  int64_t rescued_robust;   /* pairs recomputed in the FP64 32-row-strip tier */
+  int64_t h2d_bytes;
+  int64_t d2h_bytes;
+  int64_t kernel_launches;  /* kernels of this library launched */
+  double kernel_ms;         /* device time of the DP kernels (CUDA events) */
+  double total_ms;          /* host wall time of the call */
+  double host_ms;           /* host packing time */
+  int64_t live_bytes;       /* device bytes held by the call's buffers */
+  double primary_ms;        /* device time of the primary (FP32, or FP64) tier alone */
+  double rescue_ms;         /* device time of the two FP64 rescue tiers */
+} vd_stats;
+
+typedef struct vd_engine vd_engine;
+typedef struct vd_plan vd_plan;
+
+/* ---- engine --------------------------------------------------------------
+ * One engine per device and process (accelerator.py:80-103 CudaPairHMM).  It
+ * owns a stream, cached device buffers and per-parameter tables.  memory_mb
+ * bounds the device bytes of one batch; larger inputs run as several batches
+ * (accelerator.py:118-121).  Calls on one engine are serialised. */
+int vd_engine_create(int device, int64_t memory_mb, vd_engine **out);
+int vd_engine_destroy(vd_engine *engine);
+/* Name of the device, compute capability and SM count. */
+int vd_engine_info(const vd_engine *engine, char *name, int name_len, int *major, int *minor,
+                   int *sm_count);
+
+/* Score a batch (host buffers in, host out).  Replaces CudaPairHMM.score
+ * (accelerator.py:105-159): packing, transfers, the kernels and the FP64
+ * rescue all happen here.  out must hold vd_batch_outputs(batch) doubles. */
+int vd_forward(vd_engine *engine, const vd_batch *batch, const vd_params *params, double *out,
+               vd_stats *stats);
+int64_t vd_batch_outputs(const vd_batch *batch);
+
+/* ---- plans: device-resident batches --------------------------------------
+ * vd_plan_create uploads a batch and builds its work list once (ignoring the
+ * memory budget); vd_plan_run replays the kernels (captured once into a CUDA
+ * graph) on the resident inputs; vd_plan_fetch copies the results out. */
+int vd_plan_create(vd_engine *engine, const vd_batch *batch, const vd_params *params,
+                   vd_plan **out);
+int vd_plan_run(vd_plan *plan, vd_stats *stats);
+int vd_plan_fetch(vd_plan *plan, double *out);
+int vd_plan_destroy(vd_plan *plan);
+
+/* ---- drop-ins for the reference's CPU entry points -----------------------
+ * Same arguments and results as the reference functions named, computed on
+ * the default engine (device VARDEPTH_CUDA_DEVICE, default 0).  The constant
+ * gap 0.001 / ext 0.1 of the batch kernels is kept where the reference
+ * hard-codes it. */
+
+/* caller/native/caller/batch_hmm.cpp:217 pairhmm_pairs: count independent pairs,
+ * mode 0/2 semiglobal, 1 anchored; lanes is accepted and ignored. */
+int vd_pairhmm_pairs(const char *const *reads, const unsigned char *const *quals, const int *rn,
+                     const char *const *haps, const int *hn, int count, int mode, int lanes,
+                     double *out);
+/* caller/native/caller/trie_vector.cpp:284 trie_many: nr reads x nh haplotypes,
+ * out row-major by read; *cells receives the DP cells computed. */
+int vd_trie_many(const char *const *reads, const unsigned char *const *quals, const int *rn, int nr,
+                 const char *const *haps, const int *hn, int nh, int mode, int lanes, double *out,
+                 uint64_t *cells);
+/* caller/native/caller/wide.cpp:349 read_haplotype_batch_mode: one read x count
+ * haplotypes with explicit gap/ext (void in the reference; status here). */
+int vd_read_haplotype_batch_mode(const char *read, const unsigned char *qual, int n,
+                                 const char *const *haps, const int *lengths, int count, double gap,
+                                 double ext, double *out, int mode);
+/* caller/native/caller/wide.cpp:9 read_haplotype and anchored.cpp:5 anchored_pairhmm:
+ * one pair (NaN on a device error). */
+double vd_read_haplotype(const char *read, const unsigned char *qual, int n, const char *hap, int m,
+                         double gap, double ext);
+double vd_anchored_pairhmm(const char *read, const unsigned char *qual, int n, const char *hap,
+                           int m, double gap, double ext);
+
+/* ---- misc ---------------------------------------------------------------- */
+const char *vd_last_error(void);
+/* FP32 FMA throughput of a device in TFLOP/s (2 flops per FMA), measured with
+ * a register-resident FMA loop: the denominator of the FP32-pipe roofline. */
+int vd_measure_fp32_peak(int device, double *tflops);
+int vd_device_count(void);
+const char *vd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VARDEPTH_PAIRHMM_H */

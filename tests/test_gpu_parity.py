@@ -1,0 +1,266 @@
+"""Parity of the CUDA PairHMM with the reference's own results and the FP64 oracle.
+
+Tolerances:
+  * precision='float64': 2e-9 in ln, the reference's FP64 CUDA-vs-CPU bound
+    (caller/native/caller/tests/test_accelerator.py:50);
+  * precision='mixed' (FP32 scaled + FP64 rescue): |delta log10 L| <= 1e-4 per
+    pair, i.e. 2.303e-4 in ln, and identical genotype-likelihood argmax.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import FP64_ATOL_LN, LN10, MIXED_ATOL_LN, golden, golden_pairs
+from oracle import oracle as O
+from vardepth_b200 import native
+from vardepth_b200 import synthetic as S
+from vardepth_b200.accelerator import CudaPairHMM, score_many, score_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mixed():
+    return CudaPairHMM(memory_mb=4096, precision="mixed")
+
+
+@pytest.fixture(scope="module")
+def fp64():
+    return CudaPairHMM(memory_mb=4096, precision="float64")
+
+
+def _with(engine, gap, ext):
+    engine.gap, engine.ext = float(gap), float(ext)
+    return engine
+
+
+def diploid_gl(ll_rows: np.ndarray) -> np.ndarray:
+    """Unordered-genotype log-likelihoods of one region (caller/native/caller/triangular.py:27-30
+    over molecule_rows.py:10 normalised rows): sum_reads ln((L_a + L_b)/2)."""
+    v = np.exp(ll_rows - ll_rows.max(axis=1, keepdims=True))
+    H = v.shape[1]
+    a, b = np.array([(a, b) for b in range(H) for a in range(b + 1)]).T
+    return np.log(np.maximum(1e-300, (v[:, a] + v[:, b]) / 2)).sum(axis=0)
+
+
+def assert_mixed_close(got, want):
+    finite = np.isfinite(want)
+    assert np.array_equal(np.isneginf(got), np.isneginf(want))
+    err = np.abs(got[finite] - want[finite]) / LN10
+    assert err.size == 0 or err.max() <= 1e-4, f"max |dlog10| {err.max():.3e}"
+    return err
+
+
+@pytest.mark.parametrize("anchored", [False, True])
+def test_fp64_matches_reference_cpu_pairs(fp64, anchored):
+    d = golden("accel_seed31")
+    got = _with(fp64, 0.001, 0.1).score(golden_pairs(d), anchored)
+    np.testing.assert_allclose(got, d["anchored" if anchored else "semiglobal"], atol=FP64_ATOL_LN, rtol=0)
+
+
+@pytest.mark.parametrize("anchored", [False, True])
+@pytest.mark.parametrize("name", ["accel_seed31", "accel_seed17391"])
+def test_mixed_matches_reference_cpu_pairs(mixed, name, anchored):
+    d = golden(name)
+    got = _with(mixed, 0.001, 0.1).score(golden_pairs(d), anchored)
+    assert_mixed_close(got, d["anchored" if anchored else "semiglobal"])
+    if name == "accel_seed17391":
+        # random reads against random haplotypes underflow FP32: they must be rescued
+        assert mixed.last["float64_fallback_pairs"] >= 12
+        assert mixed.last["precision"] == "mixed"
+
+
+def test_base_model_pair_scores(mixed, fp64):
+    d = golden("base_seed712")
+    pairs = golden_pairs(d)
+    np.testing.assert_allclose(_with(fp64, 0.001, 0.1).score(pairs), d["semiglobal"], atol=FP64_ATOL_LN, rtol=0)
+    assert_mixed_close(_with(mixed, 0.001, 0.1).score(pairs), d["semiglobal"])
+
+
+def test_anchored_catalog(mixed, fp64):
+    d = golden("catalog_seed7713")
+    pairs = golden_pairs(d)
+    np.testing.assert_allclose(_with(fp64, 0.001, 0.1).score(pairs, True), d["anchored"], atol=1e-11, rtol=0)
+    assert_mixed_close(_with(mixed, 0.001, 0.1).score(pairs, True), d["anchored"])
+
+
+@pytest.mark.parametrize("anchored", [False, True])
+def test_edge_cases(mixed, fp64, anchored):
+    d = golden("edge_cases")
+    pairs = golden_pairs(d)
+    want = d["anchored" if anchored else "semiglobal"]
+    np.testing.assert_allclose(_with(fp64, 0.001, 0.1).score(pairs, anchored), want, atol=FP64_ATOL_LN, rtol=0)
+    assert_mixed_close(_with(mixed, 0.001, 0.1).score(pairs, anchored), want)
+    empty = _with(mixed, 0.001, 0.1).score([("", [], "A"), ("A", [30], ""), ("", [], "")], anchored)
+    assert np.isneginf(empty).all()
+
+
+@pytest.mark.parametrize("name", ["config0_q45", "config0_q30"])
+def test_config0_against_reference(mixed, name):
+    d = golden(name)
+    packed = native.Packed(d["read_bases"], d["read_quals"], d["read_off"], d["hap_bases"], d["hap_off"],
+                           region_read_off=d["region_read_off"], region_hap_off=d["region_hap_off"])
+    got = _with(mixed, d["gap"], d["ext"]).score_packed(packed)
+    want = d["semiglobal"]
+    assert_mixed_close(got, want)
+    H = int(d["region_hap_off"][1])
+    assert np.argmax(diploid_gl(got.reshape(-1, H))) == np.argmax(diploid_gl(want.reshape(-1, H)))
+
+
+def _oracle_workload(w, anchored=False):
+    pr, ph = w.explicit_pairs()
+    return O.forward_pairs(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off, pr, ph, w.gap, w.ext,
+                           anchored, O.SEMIGLOBAL_POW2, threads=0)
+
+
+def _packed(w):
+    return native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
+                         region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
+
+
+def _argmax_agree(w, got, want):
+    o = 0
+    agree = total = 0
+    for g in range(w.n_regions):
+        nr = int(w.region_read_off[g + 1] - w.region_read_off[g])
+        nh = int(w.region_hap_off[g + 1] - w.region_hap_off[g])
+        k = nr * nh
+        if k:
+            total += 1
+            agree += int(np.argmax(diploid_gl(got[o:o + k].reshape(nr, nh))) ==
+                         np.argmax(diploid_gl(want[o:o + k].reshape(nr, nh))))
+        o += k
+    return agree, total
+
+
+@pytest.mark.parametrize("anchored", [False, True])
+def test_config1_sample_against_oracle(mixed, anchored):
+    w = S.config1(n_regions=24)
+    got = _with(mixed, w.gap, w.ext).score_packed(_packed(w), anchored)
+    want = _oracle_workload(w, anchored)
+    err = assert_mixed_close(got, want)
+    agree, total = _argmax_agree(w, got, want)
+    assert agree == total
+    print(f"config1 sample anchored={anchored}: pairs {len(got)} max|dlog10| {err.max():.2e} "
+          f"p99 {np.quantile(err, .99):.2e} rescued {mixed.last['float64_fallback_pairs']}")
+
+
+def test_config2_precision_stress(mixed):
+    w = S.config2(n_regions=6)
+    got = _with(mixed, w.gap, w.ext).score_packed(_packed(w))
+    want = _oracle_workload(w)
+    err = assert_mixed_close(got, want)
+    agree, total = _argmax_agree(w, got, want)
+    assert agree == total
+    print(f"config2 sample: pairs {len(got)} max|dlog10| {err.max():.2e} rescued "
+          f"{mixed.last['float64_fallback_pairs']}/{len(got)}")
+
+
+@pytest.mark.parametrize("anchored", [False, True])
+def test_long_reads_strip_mined(mixed, fp64, anchored):
+    # reads longer than one 256-row strip, and reads just around the strip size
+    rng = np.random.default_rng(99)
+    pairs = []
+    for n, m in [(255, 300), (256, 300), (257, 300), (513, 700), (1500, 1800), (3000, 3100)]:
+        hap = "".join(rng.choice(list("ACGT"), m))
+        start = int(rng.integers(0, m - n + 1))
+        read = list(hap[start:start + n])
+        for i in np.flatnonzero(rng.random(n) < 0.03):
+            read[i] = "ACGT"[(("ACGT".index(read[i])) + 1) % 4]
+        q = rng.choice([10, 20, 30, 40], n)
+        pairs.append(("".join(read), q, hap))
+    want = np.array([O.forward(s, q.astype(np.uint8), h, 0.001, 0.1, anchored) for s, q, h in pairs])
+    np.testing.assert_allclose(_with(fp64, 0.001, 0.1).score(pairs, anchored), want, atol=FP64_ATOL_LN * 10, rtol=0)
+    assert_mixed_close(_with(mixed, 0.001, 0.1).score(pairs, anchored), want)
+
+
+def test_pairs_regions_and_chunking_agree():
+    w = S.config1(n_regions=12)
+    eng = CudaPairHMM(memory_mb=4096, gap=w.gap, ext=w.ext)
+    regions = eng.score_packed(_packed(w))
+    pr, ph = w.explicit_pairs()
+    pairs_form = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
+                               pair_read=pr, pair_hap=ph)
+    np.testing.assert_array_equal(eng.score_packed(pairs_form), regions)
+    small = CudaPairHMM(memory_mb=8, gap=w.gap, ext=w.ext)
+    chunked = small.score_packed(_packed(w))
+    assert small.last["batches"] > 1
+    np.testing.assert_array_equal(chunked, regions)
+    chunked_pairs = small.score_packed(pairs_form)
+    assert small.last["batches"] > 1
+    np.testing.assert_array_equal(chunked_pairs, regions)
+
+
+def test_plan_graph_replay_is_deterministic():
+    w = S.config1(n_regions=16)
+    eng = native.Engine(0, 4096)
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    plan = eng.plan(_packed(w), params)
+    outs = []
+    for _ in range(3):
+        st = plan.run()
+        assert st.kernel_launches == 3 and st.pairs == w.pairs()
+        outs.append(plan.fetch())
+    ref, _ = eng.forward(_packed(w), params)
+    for o in outs:
+        np.testing.assert_array_equal(o, ref)
+
+
+def test_reference_shaped_entry_points():
+    """The C-ABI drop-ins for pairhmm_pairs / trie_many / read_haplotype_batch_mode / read_haplotype."""
+    lib = native.library()
+    d = golden("accel_seed31")
+    pairs = golden_pairs(d)
+    enc = [(s.encode(), np.ascontiguousarray(q, np.uint8).tobytes(), h.encode()) for s, q, h in pairs]
+    count = len(enc)
+    reads = (ctypes.c_char_p * count)(*(e[0] for e in enc))
+    quals = (ctypes.c_char_p * count)(*(e[1] for e in enc))
+    haps = (ctypes.c_char_p * count)(*(e[2] for e in enc))
+    rn = (ctypes.c_int * count)(*(len(e[0]) for e in enc))
+    hn = (ctypes.c_int * count)(*(len(e[2]) for e in enc))
+    for mode, key in [(0, "semiglobal"), (2, "semiglobal"), (1, "anchored")]:
+        out = np.empty(count)
+        rc = lib.vd_pairhmm_pairs(reads, ctypes.cast(quals, ctypes.POINTER(native.c_u8p)), rn, haps, hn, count, mode,
+                                  8, out.ctypes.data_as(native.c_dp))
+        assert rc == 0
+        assert_mixed_close(out, d[key])
+    # trie_many: reads x haplotypes of config0 at the production constants
+    g = golden("config0_q30")
+    nr, nh = len(g["read_off"]) - 1, len(g["hap_off"]) - 1
+    rb = [bytes(g["read_bases"][g["read_off"][i]:g["read_off"][i + 1]]) for i in range(nr)]
+    qb = [bytes(g["read_quals"][g["read_off"][i]:g["read_off"][i + 1]]) for i in range(nr)]
+    hb = [bytes(g["hap_bases"][g["hap_off"][i]:g["hap_off"][i + 1]]) for i in range(nh)]
+    out = np.empty(nr * nh)
+    cells = ctypes.c_uint64()
+    rc = lib.vd_trie_many((ctypes.c_char_p * nr)(*rb), ctypes.cast((ctypes.c_char_p * nr)(*qb),
+                          ctypes.POINTER(native.c_u8p)), (ctypes.c_int * nr)(*map(len, rb)), nr,
+                          (ctypes.c_char_p * nh)(*hb), (ctypes.c_int * nh)(*map(len, hb)), nh, 0, 0,
+                          out.ctypes.data_as(native.c_dp), ctypes.byref(cells))
+    assert rc == 0 and cells.value == sum(map(len, rb)) * sum(map(len, hb))
+    assert_mixed_close(out, g["semiglobal"])
+    # read_haplotype_batch_mode with the benchmark's gap/ext
+    q45 = golden("config0_q45")
+    s0 = rb[0]
+    q0 = (ctypes.c_ubyte * len(qb[0]))(*qb[0])
+    out2 = np.empty(nh)
+    lib.vd_read_haplotype_batch_mode(s0, q0, len(s0), (ctypes.c_char_p * nh)(*hb), (ctypes.c_int * nh)(*map(len, hb)),
+                                     nh, float(q45["gap"]), float(q45["ext"]), out2.ctypes.data_as(native.c_dp), 0)
+    assert_mixed_close(out2, q45["semiglobal"][:nh])
+    single = lib.vd_read_haplotype(s0, q0, len(s0), hb[0], len(hb[0]), float(q45["gap"]), float(q45["ext"]))
+    assert abs(single - q45["semiglobal"][0]) / LN10 <= 1e-4
+    anch = lib.vd_anchored_pairhmm(s0, q0, len(s0), hb[0], len(hb[0]), 0.001, 0.1)
+    assert abs(anch - O.forward(s0, qb[0], hb[0], 0.001, 0.1, True, 0)) / LN10 <= 1e-4
+
+
+def test_score_pairs_and_many_module_api(monkeypatch):
+    monkeypatch.setenv("VARDEPTH_PAIRHMM_BACKEND", "cuda")
+    reads = ["ACGT" * 8, "A" * 30, "GATTACA"]
+    quals = [[30] * len(x) for x in reads]
+    haps = ["TT" + r + "GG" for r in reads] + ["ACGT" * 10]
+    got = score_many(reads, quals, haps)
+    want = np.array([[O.forward(r, np.array(q, np.uint8), h) for h in haps] for r, q in zip(reads, quals)])
+    assert got.shape == (3, 4)
+    assert_mixed_close(got.ravel(), want.ravel())
+    flat = score_pairs([(r, q, h) for r, q in zip(reads, quals) for h in haps])
+    np.testing.assert_array_equal(flat, got.ravel())

@@ -1,0 +1,90 @@
+"""Host-side logic of the drop-in (no GPU): input guards, packing, backend choice, workloads."""
+import numpy as np
+import pytest
+
+from vardepth_b200 import accelerator as A
+from vardepth_b200 import synthetic as S
+
+
+def test_input_guards():
+    # caller/native/caller/tests/test_accelerator.py:29-32
+    for pairs in [[("A", [256], "A")], [("A", [-1], "A")], [("A", [3.5], "A")], [("A", [], "A")], [("X", [30], "A")]]:
+        with pytest.raises(ValueError):
+            A.validate_pairs(pairs)
+    with pytest.raises(ValueError):
+        A.score_pairs([("A", [30], "A")], selection="fake")
+    with pytest.raises(ValueError):
+        A.validate_pairs([("a", [30], "A")])
+    with pytest.raises(ValueError):
+        A.validate_pairs([("A", [np.nan], "A")])
+
+
+def test_cpu_backend_is_not_provided():
+    with pytest.raises(RuntimeError, match="CPU"):
+        A.score_pairs([("A", [30], "A")], selection="cpu")
+    with pytest.raises(RuntimeError, match="CPU"):
+        A.score_many(["A"], [[30]], ["A"], selection="cpu")
+
+
+def test_backend_env(monkeypatch):
+    monkeypatch.setenv("VARDEPTH_PAIRHMM_BACKEND", "bogus")
+    with pytest.raises(ValueError):
+        A.backend()
+    monkeypatch.setenv("VARDEPTH_PAIRHMM_BACKEND", "auto")
+    assert A.backend() == "auto"
+    monkeypatch.delenv("VARDEPTH_PAIRHMM_BACKEND")
+    assert A.backend() == "cuda"
+
+
+def test_empty_batches_need_no_device():
+    assert A.score_pairs([]).shape == (0,)
+    assert A.score_many([], [], ["ACGT"]).shape == (0, 1)
+    assert A.score_many(["ACGT"], [[30] * 4], []).shape == (1, 0)
+
+
+def test_pack_pairs_layout_and_dedupe():
+    pairs = A.validate_pairs([("ACNT", [0, 20, 60, 255], "GATTACA"), ("G", [3], "G"), ("TGA", [10, 20, 30], "ACTG"),
+                              ("ACNT", [0, 20, 60, 255], "G"), ("", [], "A")])
+    pk = A.pack_pairs(pairs)
+    assert pk.batch.n_reads == 4 and pk.batch.n_haps == 4      # one ACNT read stored once
+    assert list(pk.pair_read) == [0, 1, 2, 0, 3] and list(pk.pair_hap) == [0, 1, 2, 1, 3]
+    assert bytes(pk.read_bases).decode() == "ACNTGTGA"
+    assert list(pk.read_quals) == [0, 20, 60, 255, 3, 10, 20, 30]
+    assert list(pk.read_off) == [0, 4, 5, 8, 8]
+    assert bytes(pk.hap_bases).decode() == "GATTACAGACTGA"
+    assert pk.n_outputs() == 5
+    assert all(a.flags.c_contiguous for a in (pk.read_bases, pk.read_quals, pk.read_off, pk.hap_bases, pk.hap_off))
+
+
+def test_quality_objects_are_validated_once_and_kept():
+    q = bytes([30] * 4)
+    out = A.validate_pairs([("ACGT", q, "ACGT"), ("ACGT", q, "TTTT")])
+    assert out[0][1] is out[1][1] and out[0][1].dtype == np.uint8
+
+
+def test_config0_shape():
+    w = S.config0()
+    assert w.n_regions == 1 and len(w.read_off) - 1 == 64 and list(w.hap_lengths()) == [300, 297]
+    assert set(np.unique(w.read_quals)) <= {10, 20, 30, 40}
+    assert w.pairs() == 128 and w.cells() == 64 * 150 * 597
+    assert abs(w.gap - 10 ** -4.5) < 1e-18 and w.ext == 0.1
+
+
+def test_config1_shape_small():
+    w = S.config1(n_regions=40)
+    nh = np.diff(w.region_hap_off)
+    nr = np.diff(w.region_read_off)
+    assert nh.min() >= 2 and nh.max() <= 16 and nr.min() >= 10 and nr.max() <= 500
+    rl = w.read_lengths()
+    assert rl.min() >= 1 and rl.max() <= 250
+    pr, ph = w.explicit_pairs()
+    assert len(pr) == w.pairs()
+    cells = int(np.sum(rl[pr].astype(np.int64) * w.hap_lengths()[ph]))
+    assert cells == w.cells()
+    sub = w.subset([3, 1])
+    assert sub.n_regions == 2 and sub.pairs() == nr[3] * nh[3] + nr[1] * nh[1]
+
+
+def test_workloads_are_seeded():
+    a, b = S.config1(n_regions=5), S.config1(n_regions=5)
+    assert np.array_equal(a.read_bases, b.read_bases) and np.array_equal(a.hap_bases, b.hap_bases)

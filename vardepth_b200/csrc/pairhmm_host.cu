@@ -1,0 +1,1211 @@
+// Host side of the B200 PairHMM: engine, work-list construction, memory-budget
+// batching, tier orchestration (FP32 -> FP64 -> FP64 32-row strips), CUDA
+// graph replay of resident plans, and the C ABI declared in
+// include/vardepth_pairhmm.h.
+//
+// Dispatch semantics follow caller/native/caller/accelerator.py:105-159
+// (CudaPairHMM.score): validate, bucket, chunk by a device-memory budget,
+// transfer, launch, copy back, and re-score the pairs the reduced-precision
+// pass could not resolve.  Here the re-scoring runs on the GPU as two further
+// kernel tiers fed by device-side lists, so a batch needs no host round trip.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/vardepth_pairhmm.h"
+#include "pairhmm_core.cuh"
+#include "pairhmm_launch.h"
+
+using namespace vd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(VD_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define VD_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t vd_err_ = (call);                       \
+    if (vd_err_ != cudaSuccess) return cuda_fail(vd_err_, #call); \
+  } while (0)
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// ---- model tables -----------------------------------------------------------
+
+int quality_bin(unsigned q) {
+  if (q < 15u) return 0;
+  if (q < 25u) return 1;
+  if (q < 35u) return 2;
+  return 3;
+}
+
+struct TableSet {
+  Tables<float> f32;
+  Tables<double> f64;
+  Scalars<float> s32;
+  Scalars<double> s64;
+};
+
+// Per-quality factors of the scaled recurrence (pairhmm_core.cuh).  The error
+// of a Phred byte is 10^(-min(q,60)/10) (accelerator.py:23), optionally
+// shifted by the bin offset.
+void build_tables(double g, double x, const double* offsets, TableSet* ts) {
+  const double a = 1.0 - 2.0 * g, b = 1.0 - x, alpha = 0.25 * g;
+  const double k1 = b * alpha / a, k2 = b * g / a, x4 = 0.25 * x;
+  for (int q = 0; q < 256; ++q) {
+    double phred = (double)std::min(q, 60);
+    if (offsets) phred = std::max(0.0, phred + offsets[quality_bin((unsigned)q)]);
+    const double e = std::pow(10.0, -phred / 10.0);
+    const double p1 = 1.0 - e, p0 = e / 3.0;
+    const double mx = std::max(p1, p0);
+    const double N = a * mx, f = 1.0 / N;
+    const double hit = p1 / mx, miss = p0 / mx, K = k1 * f, X = x4 * f, A = alpha * f;
+    ts->f32.hit[q] = (float)hit;  ts->f64.hit[q] = hit;
+    ts->f32.miss[q] = (float)miss; ts->f64.miss[q] = miss;
+    ts->f32.K[q] = (float)K;      ts->f64.K[q] = K;
+    ts->f32.X[q] = (float)X;      ts->f64.X[q] = X;
+    ts->f32.A[q] = (float)A;      ts->f64.A[q] = A;
+    ts->f32.lnN[q] = std::log(N); ts->f64.lnN[q] = std::log(N);
+    const unsigned char gen = p0 > p1 ? 1 : 0;
+    ts->f32.general[q] = gen;     ts->f64.general[q] = gen;
+  }
+  ts->s32.k2 = (float)k2; ts->s32.x = (float)x; ts->s32.gfin = (float)g;
+  ts->s32.c = std::ldexp(1.0f, 100); ts->s32.ln_c = 100.0 * std::log(2.0);
+  ts->s32.strip_floor = std::ldexp(1.0f, -40); ts->s32.final_floor = std::ldexp(1.0f, -64);
+  ts->s32.target_log2 = 100;
+  ts->s64.k2 = k2; ts->s64.x = x; ts->s64.gfin = g;
+  ts->s64.c = std::ldexp(1.0, 600); ts->s64.ln_c = 600.0 * std::log(2.0);
+  ts->s64.strip_floor = std::ldexp(1.0, -800); ts->s64.final_floor = std::ldexp(1.0, -900);
+  ts->s64.target_log2 = 600;
+}
+
+struct TableKey {
+  double g, x, off[4];
+  bool has_off;
+  bool operator==(const TableKey& o) const {
+    if (g != o.g || x != o.x || has_off != o.has_off) return false;
+    if (has_off) for (int i = 0; i < 4; ++i) if (off[i] != o.off[i]) return false;
+    return true;
+  }
+};
+
+// ---- device buffers -----------------------------------------------------------
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  int reserve(size_t n) {
+    if (n <= bytes) return VD_OK;
+    if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(VD_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
+    bytes = n;
+    return VD_OK;
+  }
+};
+
+}  // namespace
+
+// ---- engine -----------------------------------------------------------------------
+
+struct vd_engine {
+  int device = 0;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  char name[256] = {0};
+  size_t budget = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
+  std::mutex mu;
+  int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
+  // table cache
+  TableKey tkey{};
+  bool tvalid = false;
+  TableSet* htab = nullptr;   // pinned host copy
+  DevBuf dtab;
+  // batch arena reused by vd_forward
+  DevBuf arena;
+  std::vector<double> out_stage;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; cudaSetDevice(dev); }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+int ensure_tables(vd_engine* e, const vd_params* p) {
+  TableKey k{};
+  k.g = p->gap; k.x = p->ext; k.has_off = p->quality_offsets != nullptr;
+  if (k.has_off) for (int i = 0; i < 4; ++i) k.off[i] = p->quality_offsets[i];
+  if (e->tvalid && k == e->tkey) return VD_OK;
+  build_tables(p->gap, p->ext, p->quality_offsets, e->htab);
+  int rc = e->dtab.reserve(sizeof(TableSet));
+  if (rc) return rc;
+  VD_CUDA(cudaMemcpyAsync(e->dtab.p, e->htab, sizeof(TableSet), cudaMemcpyHostToDevice, e->stream));
+  VD_CUDA(cudaStreamSynchronize(e->stream));
+  e->tkey = k;
+  e->tvalid = true;
+  return VD_OK;
+}
+
+int validate_params(const vd_params* p) {
+  if (!p) return fail(VD_EINVAL, "params is NULL");
+  if (!(p->gap >= 0.0 && p->gap < 0.5)) return fail(VD_EINVAL, "gap must lie in [0, 0.5)");
+  if (!(p->ext >= 0.0 && p->ext < 1.0)) return fail(VD_EINVAL, "ext must lie in [0, 1)");
+  if (p->anchored != 0 && p->anchored != 1) return fail(VD_EINVAL, "anchored must be 0 or 1");
+  if (p->precision != VD_PRECISION_MIXED && p->precision != VD_PRECISION_FLOAT64)
+    return fail(VD_EINVAL, "unknown precision");
+  if (p->quality_offsets)
+    for (int i = 0; i < 4; ++i)
+      if (!std::isfinite(p->quality_offsets[i])) return fail(VD_EINVAL, "quality offsets must be finite");
+  for (int i = 0; i < 4; ++i) if (p->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  return VD_OK;
+}
+
+bool offsets_ok(const int64_t* off, int64_t n) {
+  if (n < 0 || !off) return false;
+  if (off[0] < 0) return false;
+  for (int64_t i = 0; i < n; ++i) if (off[i + 1] < off[i] || off[i + 1] - off[i] > (1 << 28)) return false;
+  return true;
+}
+
+int validate_batch(const vd_batch* b) {
+  if (!b) return fail(VD_EINVAL, "batch is NULL");
+  if (b->n_reads < 0 || b->n_haps < 0) return fail(VD_EINVAL, "negative counts");
+  if (b->n_reads > INT32_MAX - 1 || b->n_haps > INT32_MAX - 1) return fail(VD_EINVAL, "too many reads or haplotypes");
+  if (!offsets_ok(b->read_off, b->n_reads)) return fail(VD_EINVAL, "read offsets must be non-decreasing (lengths <= 2^28)");
+  if (!offsets_ok(b->hap_off, b->n_haps)) return fail(VD_EINVAL, "haplotype offsets must be non-decreasing (lengths <= 2^28)");
+  if (b->read_off[b->n_reads] > b->read_off[0] && (!b->read_bases || !b->read_quals))
+    return fail(VD_EINVAL, "read buffers are NULL");
+  if (b->hap_off[b->n_haps] > b->hap_off[0] && !b->hap_bases) return fail(VD_EINVAL, "haplotype buffer is NULL");
+  if (b->pair_read) {
+    if (!b->pair_hap || b->n_pairs < 0) return fail(VD_EINVAL, "pair arrays inconsistent");
+    for (int64_t p = 0; p < b->n_pairs; ++p)
+      if (b->pair_read[p] < 0 || b->pair_read[p] >= b->n_reads || b->pair_hap[p] < 0 || b->pair_hap[p] >= b->n_haps)
+        return fail(VD_EINVAL, "pair index out of range");
+  } else {
+    if (b->n_regions < 0 || !b->region_read_off || !b->region_hap_off) return fail(VD_EINVAL, "region arrays missing");
+    for (int64_t g = 0; g < b->n_regions; ++g) {
+      if (b->region_read_off[g + 1] < b->region_read_off[g] || b->region_hap_off[g + 1] < b->region_hap_off[g])
+        return fail(VD_EINVAL, "region offsets must be non-decreasing");
+    }
+    if (b->n_regions > 0) {
+      if (b->region_read_off[0] < 0 || b->region_read_off[b->n_regions] > b->n_reads ||
+          b->region_hap_off[0] < 0 || b->region_hap_off[b->n_regions] > b->n_haps)
+        return fail(VD_EINVAL, "region offsets out of range");
+    }
+  }
+  return VD_OK;
+}
+
+int64_t batch_outputs(const vd_batch* b) {
+  if (b->pair_read) return b->n_pairs;
+  int64_t total = 0;
+  for (int64_t g = 0; g < b->n_regions; ++g)
+    total += (b->region_read_off[g + 1] - b->region_read_off[g]) * (b->region_hap_off[g + 1] - b->region_hap_off[g]);
+  return total;
+}
+
+// Rows per lane for a read of n bases: the smallest R with 32 R >= n, at most
+// 8; longer reads are strip-mined in strips of 256 rows.
+int rows_per_lane(int n) { return std::min(kMaxR, std::max(1, (n + kWarp - 1) / kWarp)); }
+
+// ---- host plan ------------------------------------------------------------------
+
+// A chunk of a batch laid out the way the kernels read it.
+struct HostChunk {
+  // reads [ra, rb) and haplotypes [ha, hb) of the batch (global indices)
+  int64_t ra = 0, rb = 0, ha = 0, hb = 0;
+  std::vector<int64_t> read_off;   // rebased, rb - ra + 1
+  std::vector<int32_t> read_code;
+  std::vector<int64_t> hap_off;    // rebased, hb - ha + 1
+  std::vector<WorkItem> items;
+  std::vector<int32_t> hap_sel;    // pair form
+  std::vector<int64_t> out_sel;    // pair form (chunk-local output slots)
+  std::vector<int64_t> out_global; // pair form: batch output index of each local slot
+  int64_t out_begin = 0;           // region form: first batch output slot
+  int64_t n_out = 0;
+  int64_t cells = 0;
+  int64_t pairs_scored = 0;
+  int max_hap = 0;
+  bool any_long = false;           // a read longer than 32 (the robust tier strip-mines it)
+  bool any_strip = false;          // a read longer than one 256-row strip (every tier strip-mines it)
+};
+
+// The robust tier runs on a small grid: it only sees pairs the FP64 wavefront
+// could not resolve, and its strip scratch then stays small.
+constexpr int kRobustBlocks = 32;
+
+// Sort items by decreasing cost so that the persistent warps finish together
+// (longest-processing-time first), with an O(n) bucket pass.
+void order_items(std::vector<WorkItem>& items, const std::vector<int64_t>& cost) {
+  const int nb = 256;
+  std::vector<int64_t> count(nb + 1, 0);
+  std::vector<int> key(items.size());
+  for (size_t i = 0; i < items.size(); ++i) {
+    const double c = (double)std::max<int64_t>(1, cost[i]);
+    int k = (int)(std::log2(c) * 4.0);
+    k = std::max(0, std::min(nb - 1, k));
+    key[i] = nb - 1 - k;  // descending
+    ++count[key[i] + 1];
+  }
+  for (int k = 0; k < nb; ++k) count[k + 1] += count[k];
+  std::vector<WorkItem> out(items.size());
+  for (size_t i = 0; i < items.size(); ++i) out[count[key[i]]++] = items[i];
+  items.swap(out);
+}
+
+struct ReadInfo {
+  int n;
+  int32_t code;
+};
+
+ReadInfo read_info(const vd_batch* b, int64_t r) {
+  const int64_t o = b->read_off[r];
+  const int n = (int)(b->read_off[r + 1] - o);
+  ReadInfo ri{n, 0};
+  if (n <= 0) return ri;
+  bool gen = false;
+  const unsigned char* q = b->read_quals + o;
+  for (int i = 0; i < n; ++i) {
+    // P0 > P1 only for Phred 0 and 1 (e > 0.75); offsets can move a bin there
+    if (q[i] < 2) { gen = true; break; }
+  }
+  const int R = rows_per_lane(n);
+  ri.code = make_code(R, (n - 1) % R, gen, n > kStripRows);
+  return ri;
+}
+
+// Quality offsets can push bins into the P0 > P1 regime; recompute the
+// general flag from the tables in that case.
+bool read_general(const vd_batch* b, int64_t r, const TableSet* ts) {
+  const int64_t o = b->read_off[r];
+  const int n = (int)(b->read_off[r + 1] - o);
+  for (int i = 0; i < n; ++i) if (ts->f64.general[b->read_quals[o + i]]) return true;
+  return false;
+}
+
+void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bool offsets) {
+  c.read_off.resize(c.rb - c.ra + 1);
+  c.read_code.resize(c.rb - c.ra);
+  const int64_t r0 = b->read_off[c.ra];
+  for (int64_t r = c.ra; r <= c.rb; ++r) c.read_off[r - c.ra] = b->read_off[r] - r0;
+  for (int64_t r = c.ra; r < c.rb; ++r) {
+    ReadInfo ri = read_info(b, r);
+    if (offsets && ri.n > 0 && !code_general(ri.code) && read_general(b, r, ts))
+      ri.code |= 256;
+    c.read_code[r - c.ra] = ri.code;
+    if (ri.n > kWarp) c.any_long = true;
+    if (ri.n > kStripRows) c.any_strip = true;
+  }
+  c.hap_off.resize(c.hb - c.ha + 1);
+  const int64_t h0 = b->hap_off[c.ha];
+  for (int64_t h = c.ha; h <= c.hb; ++h) c.hap_off[h - c.ha] = b->hap_off[h] - h0;
+  c.max_hap = 0;
+  for (int64_t h = c.ha; h < c.hb; ++h) c.max_hap = std::max<int>(c.max_hap, (int)(b->hap_off[h + 1] - b->hap_off[h]));
+}
+
+// Work items of a region chunk: one item per read with the region's non-empty
+// haplotypes as contiguous runs; reads longer than a strip get one item per
+// haplotype (their strip boundary scratch holds one haplotype).
+void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSet* ts, bool offsets,
+                        HostChunk& c) {
+  c.ra = b->region_read_off[g0];
+  c.rb = b->region_read_off[g1];
+  c.ha = b->region_hap_off[g0];
+  c.hb = b->region_hap_off[g1];
+  c.out_begin = 0;
+  for (int64_t g = 0; g < g0; ++g)
+    c.out_begin += (b->region_read_off[g + 1] - b->region_read_off[g]) * (b->region_hap_off[g + 1] - b->region_hap_off[g]);
+  finish_chunk_common(c, b, ts, offsets);
+  std::vector<int64_t> cost;
+  int64_t out = 0;
+  const int kMaxStream = 1 << 30;
+  for (int64_t g = g0; g < g1; ++g) {
+    const int64_t r_lo = b->region_read_off[g], r_hi = b->region_read_off[g + 1];
+    const int64_t h_lo = b->region_hap_off[g], h_hi = b->region_hap_off[g + 1];
+    const int64_t nh = h_hi - h_lo;
+    for (int64_t r = r_lo; r < r_hi; ++r, out += nh) {
+      const int32_t code = c.read_code[r - c.ra];
+      const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
+      if (n <= 0) continue;
+      const int R = code_R(code);
+      const int64_t rows = (int64_t)kWarp * R * ((n + kWarp * R - 1) / (kWarp * R));
+      const bool multistrip = n > kStripRows;
+      int64_t h = h_lo;
+      while (h < h_hi) {
+        const int m0 = (int)(b->hap_off[h + 1] - b->hap_off[h]);
+        if (m0 <= 0) { ++h; continue; }
+        int64_t run_end = h, stream = 0;
+        while (run_end < h_hi) {
+          const int m = (int)(b->hap_off[run_end + 1] - b->hap_off[run_end]);
+          if (m <= 0) break;
+          if (run_end > h && (multistrip || stream + m + 1 > kMaxStream)) break;
+          stream += m + 1;
+          c.cells += (int64_t)n * m;
+          ++c.pairs_scored;
+          ++run_end;
+        }
+        WorkItem w;
+        w.read = (int32_t)(r - c.ra);
+        w.nhap = (int32_t)(run_end - h);
+        w.hap_begin = h - c.ha;
+        w.out_begin = out + (h - h_lo);
+        w.code = code;
+        w.tier = 0;
+        c.items.push_back(w);
+        cost.push_back(rows * (stream + kWarp));
+        h = run_end;
+      }
+    }
+  }
+  c.n_out = out;
+  order_items(c.items, cost);
+}
+
+// Pair form: pairs grouped by read (counting sort), each read's haplotypes as
+// an indirect list.
+struct PairGroups {
+  std::vector<int64_t> start;  // per read, n_reads + 1
+  std::vector<int64_t> order;  // pair indices grouped by read
+};
+
+void group_pairs(const vd_batch* b, PairGroups& pg) {
+  pg.start.assign(b->n_reads + 1, 0);
+  for (int64_t p = 0; p < b->n_pairs; ++p) ++pg.start[b->pair_read[p] + 1];
+  for (int64_t r = 0; r < b->n_reads; ++r) pg.start[r + 1] += pg.start[r];
+  std::vector<int64_t> fill(pg.start.begin(), pg.start.end() - 1);
+  pg.order.resize(b->n_pairs);
+  for (int64_t p = 0; p < b->n_pairs; ++p) pg.order[fill[b->pair_read[p]]++] = p;
+}
+
+void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64_t rb, const TableSet* ts,
+                      bool offsets, HostChunk& c) {
+  c.ra = ra;
+  c.rb = rb;
+  c.ha = 0;
+  c.hb = b->n_haps;
+  finish_chunk_common(c, b, ts, offsets);
+  std::vector<int64_t> cost;
+  const int kMaxStream = 1 << 30;
+  for (int64_t r = ra; r < rb; ++r) {
+    const int32_t code = c.read_code[r - ra];
+    const int n = (int)(c.read_off[r - ra + 1] - c.read_off[r - ra]);
+    const int R = code_R(code);
+    const bool multistrip = n > kStripRows;
+    const int64_t rows = n > 0 ? (int64_t)kWarp * R * ((n + kWarp * R - 1) / (kWarp * R)) : 0;
+    int64_t list_begin = (int64_t)c.hap_sel.size();
+    int64_t stream = 0;
+    auto flush = [&]() {
+      const int64_t cnt = (int64_t)c.hap_sel.size() - list_begin;
+      if (cnt <= 0) return;
+      WorkItem w;
+      w.read = (int32_t)(r - ra);
+      w.nhap = (int32_t)cnt;
+      w.hap_begin = list_begin;
+      w.out_begin = list_begin;
+      w.code = code;
+      w.tier = 0;
+      c.items.push_back(w);
+      cost.push_back(rows * (stream + kWarp));
+      list_begin = (int64_t)c.hap_sel.size();
+      stream = 0;
+    };
+    for (int64_t k = pg.start[r]; k < pg.start[r + 1]; ++k) {
+      const int64_t p = pg.order[k];
+      const int64_t h = b->pair_hap[p];
+      const int m = (int)(b->hap_off[h + 1] - b->hap_off[h]);
+      const int64_t slot = (int64_t)c.out_global.size();
+      c.out_global.push_back(p);
+      if (n <= 0 || m <= 0) {
+        // stays -inf: out_sel keeps no entry for it
+        continue;
+      }
+      if (stream > 0 && (multistrip || stream + m + 1 > kMaxStream)) flush();
+      c.hap_sel.push_back((int32_t)h);
+      c.out_sel.push_back(slot);
+      stream += m + 1;
+      c.cells += (int64_t)n * m;
+      ++c.pairs_scored;
+    }
+    flush();
+  }
+  c.n_out = (int64_t)c.out_global.size();
+  order_items(c.items, cost);
+}
+
+// Device bytes a chunk needs (inputs, lists, outputs, rescue lists, scratch).
+struct Layout {
+  size_t o_rb, o_rq, o_roff, o_rcode, o_hb, o_hoff, o_hsel, o_osel, o_items, o_out, o_sp1, o_sp2, o_cnt,
+      o_scratch, total;
+  int64_t scratch_stride;  // double2 records per warp slot
+  int64_t warps;
+};
+
+Layout layout_for(const HostChunk& c, const vd_batch* b, int64_t warps) {
+  Layout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + std::max<size_t>(bytes, 1), 256); return o; };
+  const int64_t read_bytes = c.read_off.back();
+  const int64_t hap_bytes = c.hap_off.back();
+  L.o_rb = take(read_bytes);
+  L.o_rq = take(read_bytes);
+  L.o_roff = take(c.read_off.size() * sizeof(int64_t));
+  L.o_rcode = take(c.read_code.size() * sizeof(int32_t));
+  L.o_hb = take(hap_bytes);
+  L.o_hoff = take(c.hap_off.size() * sizeof(int64_t));
+  L.o_hsel = take(c.hap_sel.size() * sizeof(int32_t));
+  L.o_osel = take(c.out_sel.size() * sizeof(int64_t));
+  L.o_items = take(c.items.size() * sizeof(WorkItem));
+  L.o_out = take((size_t)c.n_out * sizeof(double));
+  L.o_sp1 = take((size_t)std::max<int64_t>(1, c.pairs_scored) * sizeof(RescueEntry));
+  L.o_sp2 = take((size_t)std::max<int64_t>(1, c.pairs_scored) * sizeof(RescueEntry));
+  L.o_cnt = take(16 * sizeof(unsigned long long));
+  L.scratch_stride = c.any_long ? (int64_t)c.max_hap + 1 : 0;
+  L.warps = c.any_strip ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
+  L.o_scratch = take((size_t)std::max<int64_t>(1, L.scratch_stride) * warps * sizeof(double2));
+  L.total = off;
+  (void)b;
+  return L;
+}
+
+__global__ void fill_kernel(double* p, int64_t n, double v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+}  // namespace
+
+// ---- plan -----------------------------------------------------------------------
+
+struct vd_plan {
+  vd_engine* eng = nullptr;
+  DevBuf own;              // buffers of a standalone plan
+  char* base = nullptr;    // device base of the layout
+  Layout L{};
+  HostChunk chunk;
+  vd_params params{};
+  double offsets[4] = {0, 0, 0, 0};
+  bool has_offsets = false;
+  cudaGraphExec_t graph = nullptr;
+  int64_t last_rescued1 = 0, last_rescued2 = 0;
+};
+
+namespace {
+
+BatchView batch_view(vd_plan* pl) {
+  BatchView bv{};
+  char* d = pl->base;
+  bv.read_bases = (const uint8_t*)(d + pl->L.o_rb);
+  bv.read_quals = (const uint8_t*)(d + pl->L.o_rq);
+  bv.read_off = (const int64_t*)(d + pl->L.o_roff);
+  bv.read_code = (const int32_t*)(d + pl->L.o_rcode);
+  bv.hap_bases = (const uint8_t*)(d + pl->L.o_hb);
+  bv.hap_off = (const int64_t*)(d + pl->L.o_hoff);
+  bv.hap_sel = pl->chunk.hap_sel.empty() && pl->chunk.out_sel.empty() ? nullptr : (const int32_t*)(d + pl->L.o_hsel);
+  bv.out_sel = bv.hap_sel ? (const int64_t*)(d + pl->L.o_osel) : nullptr;
+  bv.out = (double*)(d + pl->L.o_out);
+  return bv;
+}
+
+int upload_chunk(vd_plan* pl, const vd_batch* b, int64_t* h2d) {
+  vd_engine* e = pl->eng;
+  HostChunk& c = pl->chunk;
+  char* d = pl->base;
+  const int64_t read_bytes = c.read_off.back();
+  const int64_t hap_bytes = c.hap_off.back();
+  int64_t bytes = 0;
+  auto put = [&](size_t off, const void* src, size_t n) -> int {
+    if (n == 0) return VD_OK;
+    VD_CUDA(cudaMemcpyAsync(d + off, src, n, cudaMemcpyHostToDevice, e->stream));
+    bytes += (int64_t)n;
+    return VD_OK;
+  };
+  int rc;
+  if ((rc = put(pl->L.o_rb, b->read_bases + b->read_off[c.ra], read_bytes))) return rc;
+  if ((rc = put(pl->L.o_rq, b->read_quals + b->read_off[c.ra], read_bytes))) return rc;
+  if ((rc = put(pl->L.o_roff, c.read_off.data(), c.read_off.size() * sizeof(int64_t)))) return rc;
+  if ((rc = put(pl->L.o_rcode, c.read_code.data(), c.read_code.size() * sizeof(int32_t)))) return rc;
+  if ((rc = put(pl->L.o_hb, b->hap_bases + b->hap_off[c.ha], hap_bytes))) return rc;
+  if ((rc = put(pl->L.o_hoff, c.hap_off.data(), c.hap_off.size() * sizeof(int64_t)))) return rc;
+  if ((rc = put(pl->L.o_hsel, c.hap_sel.data(), c.hap_sel.size() * sizeof(int32_t)))) return rc;
+  if ((rc = put(pl->L.o_osel, c.out_sel.data(), c.out_sel.size() * sizeof(int64_t)))) return rc;
+  if ((rc = put(pl->L.o_items, c.items.data(), c.items.size() * sizeof(WorkItem)))) return rc;
+  if (c.n_out > 0) {
+    fill_kernel<<<(int)std::min<int64_t>(4096, (c.n_out + 255) / 256), 256, 0, e->stream>>>(
+        (double*)(d + pl->L.o_out), c.n_out, -HUGE_VAL);
+    VD_CUDA(cudaGetLastError());
+  }
+  if (h2d) *h2d += bytes;
+  return VD_OK;
+}
+
+// Enqueue the three tiers on the engine stream, bracketed by the engine's
+// events: ev_begin .. ev_mid is the primary tier, ev_mid .. ev_end the rescue.
+int enqueue_tiers(vd_plan* pl, int* launches) {
+  vd_engine* e = pl->eng;
+  char* d = pl->base;
+  const Layout& L = pl->L;
+  const bool anch = pl->params.anchored != 0;
+  const bool f64 = pl->params.precision == VD_PRECISION_FLOAT64;
+  unsigned long long* cnt = (unsigned long long*)(d + L.o_cnt);
+  // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag
+  VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), e->stream));
+  VD_CUDA(cudaEventRecord(e->ev_begin, e->stream));
+  const BatchView bv = batch_view(pl);
+  TableSet* dt = (TableSet*)e->dtab.p;
+  QueueView q{};
+  q.scratch = d + L.o_scratch;
+  q.scratch_stride = L.scratch_stride;
+  q.error_flag = (int*)(cnt + 5);
+  const int64_t cap = std::max<int64_t>(1, pl->chunk.pairs_scored);
+  // tier 0
+  q.items = (const WorkItem*)(d + L.o_items);
+  q.entries = nullptr;
+  q.count = nullptr;
+  q.n_items = (long long)pl->chunk.items.size();
+  q.head = cnt + 0;
+  q.spill = (RescueEntry*)(d + L.o_sp1);
+  q.spill_count = cnt + 3;
+  q.spill_cap = cap;
+  int n = 0;
+  if (!pl->chunk.items.empty()) {
+    cudaError_t err = f64 ? launch_f64(anch, bv, q, &dt->f64, dt->s64, 1, e->grid[1][anch], e->stream)
+                          : launch_f32(anch, bv, q, &dt->f32, dt->s32, 0, e->grid[0][anch], e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "primary tier launch");
+    ++n;
+    VD_CUDA(cudaEventRecord(e->ev_mid, e->stream));
+    BatchView rv = bv;
+    rv.hap_sel = nullptr;
+    rv.out_sel = nullptr;
+    QueueView q1 = q;
+    if (!f64) {
+      // tier 1: FP64 wavefront over the FP32 spills
+      q1.items = nullptr;
+      q1.entries = (const RescueEntry*)(d + L.o_sp1);
+      q1.count = cnt + 3;
+      q1.n_items = cap;
+      q1.head = cnt + 1;
+      q1.spill = (RescueEntry*)(d + L.o_sp2);
+      q1.spill_count = cnt + 4;
+      err = launch_f64(anch, rv, q1, &dt->f64, dt->s64, 1, e->grid[1][anch], e->stream);
+      if (err != cudaSuccess) return cuda_fail(err, "rescue tier launch");
+      ++n;
+    }
+    // tier 2: FP64 32-row strips over what the FP64 wavefront spilled
+    QueueView q2 = q;
+    q2.items = nullptr;
+    q2.entries = (const RescueEntry*)(d + (f64 ? L.o_sp1 : L.o_sp2));
+    q2.count = cnt + (f64 ? 3 : 4);
+    q2.n_items = cap;
+    q2.head = cnt + 2;
+    q2.spill = nullptr;
+    q2.spill_count = nullptr;
+    q2.spill_cap = 0;
+    const int robust_grid = pl->chunk.any_strip ? e->grid[1][anch] : std::min(e->grid[1][anch], kRobustBlocks);
+    err = launch_f64(anch, rv, q2, &dt->f64, dt->s64, 2, robust_grid, e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "robust tier launch");
+    ++n;
+  } else {
+    VD_CUDA(cudaEventRecord(e->ev_mid, e->stream));
+  }
+  VD_CUDA(cudaEventRecord(e->ev_end, e->stream));
+  if (launches) *launches = n;
+  return VD_OK;
+}
+
+int tier_times(vd_engine* e, double* total, double* primary, double* rescue) {
+  float a = 0.f, b = 0.f;
+  VD_CUDA(cudaEventElapsedTime(&a, e->ev_begin, e->ev_mid));
+  VD_CUDA(cudaEventElapsedTime(&b, e->ev_mid, e->ev_end));
+  *primary += a;
+  *rescue += b;
+  *total += a + b;
+  return VD_OK;
+}
+
+int read_counters(vd_plan* pl, int64_t* r1, int64_t* r2) {
+  unsigned long long h[6];
+  VD_CUDA(cudaMemcpyAsync(h, pl->base + pl->L.o_cnt, sizeof(h), cudaMemcpyDeviceToHost, pl->eng->stream));
+  VD_CUDA(cudaStreamSynchronize(pl->eng->stream));
+  if (h[5]) return fail(VD_EOVERFLOW, "rescue list overflow");
+  const bool f64 = pl->params.precision == VD_PRECISION_FLOAT64;
+  *r1 = f64 ? 0 : (int64_t)h[3];
+  *r2 = (int64_t)(f64 ? h[3] : h[4]);
+  return VD_OK;
+}
+
+int init_engine_grids(vd_engine* e) {
+  for (int f = 0; f < 2; ++f)
+    for (int a = 0; a < 2; ++a) {
+      int bps = 0;
+      cudaError_t err = f ? occupancy_f64(a != 0, &bps) : occupancy_f32(a != 0, &bps);
+      if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+      e->grid[f][a] = std::max(1, bps) * e->sm_count;
+    }
+  return VD_OK;
+}
+
+int64_t max_grid_warps(const vd_engine* e) {
+  int g = 0;
+  for (int f = 0; f < 2; ++f) for (int a = 0; a < 2; ++a) g = std::max(g, e->grid[f][a]);
+  return (int64_t)g * kWarpsPerBlock;
+}
+
+std::mutex g_default_mu;
+vd_engine* g_default = nullptr;
+
+int default_engine(vd_engine** out) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default) {
+    const char* dev = std::getenv("VARDEPTH_CUDA_DEVICE");
+    const char* mb = std::getenv("VARDEPTH_CUDA_MEMORY_MB");
+    int rc = vd_engine_create(dev ? std::atoi(dev) : 0, mb ? std::atoll(mb) : 4096, &g_default);
+    if (rc) return rc;
+  }
+  *out = g_default;
+  return VD_OK;
+}
+
+int default_precision() {
+  const char* p = std::getenv("VARDEPTH_CUDA_PRECISION");
+  if (p && std::strcmp(p, "float64") == 0) return VD_PRECISION_FLOAT64;
+  return VD_PRECISION_MIXED;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vd_last_error(void) { return g_last_error.c_str(); }
+
+const char* vd_version(void) { return "vardepth-pairhmm-b200 0.1 sm_100a"; }
+
+int vd_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n;
+}
+
+int vd_engine_create(int device, int64_t memory_mb, vd_engine** out) {
+  if (!out) return fail(VD_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (memory_mb < 8) return fail(VD_EINVAL, "CUDA workspace budget must be at least 8 MiB");
+  int count = 0;
+  cudaError_t err = cudaGetDeviceCount(&count);
+  if (err != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return fail(VD_ENODEV, "CUDA PairHMM requires an accessible NVIDIA GPU");
+  }
+  if (device < 0 || device >= count) return fail(VD_ENODEV, "CUDA device index out of range");
+  DeviceGuard guard(device);
+  cudaDeviceProp prop;
+  VD_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(VD_ENODEV, "this library is built for sm_100a (B200) only");
+  vd_engine* e = new vd_engine();
+  e->device = device;
+  e->sm_count = prop.multiProcessorCount;
+  e->cc_major = prop.major;
+  e->cc_minor = prop.minor;
+  std::snprintf(e->name, sizeof(e->name), "%s", prop.name);
+  e->budget = (size_t)memory_mb << 20;
+  int rc = VD_OK;
+  if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_mid)) != cudaSuccess ||
+      (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
+      (err = cudaMallocHost((void**)&e->htab, sizeof(TableSet))) != cudaSuccess) {
+    rc = cuda_fail(err, "engine setup");
+  }
+  if (!rc) rc = init_engine_grids(e);
+  if (rc) { vd_engine_destroy(e); return rc; }
+  *out = e;
+  return VD_OK;
+}
+
+int vd_engine_destroy(vd_engine* e) {
+  if (!e) return VD_OK;
+  {
+    DeviceGuard guard(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    e->arena.release();
+    e->dtab.release();
+    if (e->htab) cudaFreeHost(e->htab);
+    if (e->ev_begin) cudaEventDestroy(e->ev_begin);
+    if (e->ev_mid) cudaEventDestroy(e->ev_mid);
+    if (e->ev_end) cudaEventDestroy(e->ev_end);
+    if (e->stream) cudaStreamDestroy(e->stream);
+  }
+  if (e == g_default) g_default = nullptr;
+  delete e;
+  return VD_OK;
+}
+
+int vd_engine_info(const vd_engine* e, char* name, int name_len, int* major, int* minor, int* sm_count) {
+  if (!e) return fail(VD_EINVAL, "engine is NULL");
+  if (name && name_len > 0) std::snprintf(name, (size_t)name_len, "%s", e->name);
+  if (major) *major = e->cc_major;
+  if (minor) *minor = e->cc_minor;
+  if (sm_count) *sm_count = e->sm_count;
+  return VD_OK;
+}
+
+int64_t vd_batch_outputs(const vd_batch* b) {
+  if (validate_batch(b)) return -1;
+  return batch_outputs(b);
+}
+
+int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out, vd_stats* st) {
+  const double t0 = now_ms();
+  if (!e) return fail(VD_EINVAL, "engine is NULL");
+  int rc = validate_params(p);
+  if (!rc) rc = validate_batch(b);
+  if (rc) return rc;
+  const int64_t n_out = batch_outputs(b);
+  if (n_out > 0 && !out) return fail(VD_EINVAL, "out is NULL");
+  std::lock_guard<std::mutex> lk(e->mu);
+  DeviceGuard guard(e->device);
+  vd_stats s{};
+  s.pairs = n_out;
+  if ((rc = ensure_tables(e, p))) return rc;
+  const bool offsets = p->quality_offsets != nullptr;
+  const int64_t warps = max_grid_warps(e);
+
+  // chunk boundaries: regions (region form) or reads (pair form)
+  PairGroups pg;
+  const bool pair_form = b->pair_read != nullptr;
+  if (pair_form) group_pairs(b, pg);
+  const int64_t units = pair_form ? b->n_reads : b->n_regions;
+  // bytes per unit, estimated from inputs; a chunk grows until the estimate
+  // reaches the budget (accelerator.py:118-121 semantics)
+  auto unit_bytes = [&](int64_t u) -> int64_t {
+    if (pair_form) {
+      const int64_t n = b->read_off[u + 1] - b->read_off[u];
+      const int64_t np = pg.start[u + 1] - pg.start[u];
+      return 2 * n + 64 + np * (4 + 8 + 8 + 32) + 64;
+    }
+    const int64_t r0 = b->region_read_off[u], r1 = b->region_read_off[u + 1];
+    const int64_t h0 = b->region_hap_off[u], h1 = b->region_hap_off[u + 1];
+    const int64_t np = (r1 - r0) * (h1 - h0);
+    return 2 * (b->read_off[r1] - b->read_off[r0]) + (r1 - r0) * 64 + (b->hap_off[h1] - b->hap_off[h0]) +
+           (h1 - h0) * 8 + np * (8 + 32);
+  };
+  int64_t fixed = pair_form ? (b->hap_off[b->n_haps] - b->hap_off[0]) + 8 * b->n_haps : 0;
+  int64_t max_hap = 0, max_read = 0;
+  for (int64_t h = 0; h < b->n_haps; ++h) max_hap = std::max<int64_t>(max_hap, b->hap_off[h + 1] - b->hap_off[h]);
+  for (int64_t r = 0; r < b->n_reads; ++r) max_read = std::max<int64_t>(max_read, b->read_off[r + 1] - b->read_off[r]);
+  const int64_t scratch_warps = max_read > kStripRows ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
+  fixed += (max_hap + 1) * scratch_warps * (int64_t)sizeof(double2) + 64 * 1024;
+  const int64_t budget = (int64_t)e->budget;
+  int64_t u = 0;
+  std::vector<double>& stage = e->out_stage;
+  int64_t region_out_base = 0;
+  while (u < units) {
+    int64_t u_end = u, bytes = fixed;
+    while (u_end < units) {
+      const int64_t ub = unit_bytes(u_end);
+      if (u_end > u && bytes + ub > budget) break;
+      bytes += ub;
+      ++u_end;
+    }
+    if (bytes > budget) return fail(VD_ENOMEM, "One pair exceeds CUDA workspace budget");
+    const double th = now_ms();
+    vd_plan pl;
+    pl.eng = e;
+    pl.params = *p;
+    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, pl.chunk);
+    else build_region_chunk(b, u, u_end, e->htab, offsets, pl.chunk);
+    HostChunk& c = pl.chunk;
+    pl.L = layout_for(c, b, warps);
+    s.host_ms += now_ms() - th;
+    if ((rc = e->arena.reserve(pl.L.total))) return rc;
+    pl.base = (char*)e->arena.p;
+    s.live_bytes = std::max<int64_t>(s.live_bytes, (int64_t)pl.L.total);
+    if ((rc = upload_chunk(&pl, b, &s.h2d_bytes))) return rc;
+    int launches = 0;
+    if ((rc = enqueue_tiers(&pl, &launches))) return rc;
+    s.kernel_launches += launches + (c.n_out > 0 ? 1 : 0);  // the -inf fill of the upload
+    // results
+    const double* dout = (const double*)(pl.base + pl.L.o_out);
+    if (c.n_out > 0) {
+      if (pair_form) {
+        stage.resize((size_t)c.n_out);
+        VD_CUDA(cudaMemcpyAsync(stage.data(), dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+      } else {
+        VD_CUDA(cudaMemcpyAsync(out + c.out_begin, dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+      }
+      s.d2h_bytes += c.n_out * (int64_t)sizeof(double);
+    }
+    int64_t r1 = 0, r2 = 0;
+    if ((rc = read_counters(&pl, &r1, &r2))) return rc;
+    if ((rc = tier_times(e, &s.kernel_ms, &s.primary_ms, &s.rescue_ms))) return rc;
+    s.rescued_fp64 += r1;
+    s.rescued_robust += r2;
+    if (pair_form) for (int64_t k = 0; k < c.n_out; ++k) out[c.out_global[k]] = stage[k];
+    s.dp_cells += c.cells;
+    s.work_items += (int64_t)c.items.size();
+    ++s.batches;
+    region_out_base += c.n_out;
+    u = u_end;
+  }
+  s.total_ms = now_ms() - t0;
+  if (st) *st = s;
+  return VD_OK;
+}
+
+int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan** out) {
+  if (!e || !out) return fail(VD_EINVAL, "engine or out is NULL");
+  *out = nullptr;
+  int rc = validate_params(p);
+  if (!rc) rc = validate_batch(b);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(e->mu);
+  DeviceGuard guard(e->device);
+  if ((rc = ensure_tables(e, p))) return rc;
+  vd_plan* pl = new vd_plan();
+  pl->eng = e;
+  pl->params = *p;
+  if (p->quality_offsets) {
+    pl->has_offsets = true;
+    for (int i = 0; i < 4; ++i) pl->offsets[i] = p->quality_offsets[i];
+    pl->params.quality_offsets = pl->offsets;
+  }
+  const bool offsets = p->quality_offsets != nullptr;
+  if (b->pair_read) {
+    PairGroups pg;
+    group_pairs(b, pg);
+    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, pl->chunk);
+  } else {
+    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, pl->chunk);
+  }
+  pl->L = layout_for(pl->chunk, b, max_grid_warps(e));
+  if ((rc = pl->own.reserve(pl->L.total))) { delete pl; return rc; }
+  pl->base = (char*)pl->own.p;
+  if ((rc = upload_chunk(pl, b, nullptr))) { delete pl; return rc; }
+  cudaError_t err = cudaStreamSynchronize(e->stream);
+  if (err != cudaSuccess) { delete pl; return cuda_fail(err, "plan upload"); }
+  // the input buffers of the batch are no longer needed on the host side
+  *out = pl;
+  return VD_OK;
+}
+
+int vd_plan_run(vd_plan* pl, vd_stats* st) {
+  if (!pl) return fail(VD_EINVAL, "plan is NULL");
+  vd_engine* e = pl->eng;
+  const double t0 = now_ms();
+  std::lock_guard<std::mutex> lk(e->mu);
+  DeviceGuard guard(e->device);
+  int rc;
+  if ((rc = ensure_tables(e, &pl->params))) return rc;
+  int launches = 0;
+  if (!pl->graph) {
+    cudaGraph_t g = nullptr;
+    VD_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_tiers(pl, &launches);
+    cudaError_t err = cudaStreamEndCapture(e->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (err != cudaSuccess) return cuda_fail(err, "graph capture");
+    err = cudaGraphInstantiate(&pl->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess) { pl->graph = nullptr; return cuda_fail(err, "graph instantiate"); }
+  } else {
+    launches = pl->chunk.items.empty() ? 0 : (pl->params.precision == VD_PRECISION_FLOAT64 ? 2 : 3);
+  }
+  VD_CUDA(cudaGraphLaunch(pl->graph, e->stream));
+  int64_t r1 = 0, r2 = 0;
+  if ((rc = read_counters(pl, &r1, &r2))) return rc;
+  double ms = 0.0, pms = 0.0, rms = 0.0;
+  if ((rc = tier_times(e, &ms, &pms, &rms))) return rc;
+  pl->last_rescued1 = r1;
+  pl->last_rescued2 = r2;
+  if (st) {
+    vd_stats s{};
+    s.pairs = pl->chunk.n_out;
+    s.dp_cells = pl->chunk.cells;
+    s.work_items = (int64_t)pl->chunk.items.size();
+    s.batches = 1;
+    s.rescued_fp64 = r1;
+    s.rescued_robust = r2;
+    s.kernel_launches = launches;
+    s.kernel_ms = ms;
+    s.primary_ms = pms;
+    s.rescue_ms = rms;
+    s.total_ms = now_ms() - t0;
+    s.live_bytes = (int64_t)pl->L.total;
+    *st = s;
+  }
+  return VD_OK;
+}
+
+int vd_plan_fetch(vd_plan* pl, double* out) {
+  if (!pl) return fail(VD_EINVAL, "plan is NULL");
+  vd_engine* e = pl->eng;
+  const HostChunk& c = pl->chunk;
+  if (c.n_out > 0 && !out) return fail(VD_EINVAL, "out is NULL");
+  std::lock_guard<std::mutex> lk(e->mu);
+  DeviceGuard guard(e->device);
+  const double* dout = (const double*)(pl->base + pl->L.o_out);
+  if (c.n_out == 0) return VD_OK;
+  if (c.out_global.empty()) {
+    VD_CUDA(cudaMemcpyAsync(out, dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    VD_CUDA(cudaStreamSynchronize(e->stream));
+  } else {
+    std::vector<double> tmp((size_t)c.n_out);
+    VD_CUDA(cudaMemcpyAsync(tmp.data(), dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    VD_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t k = 0; k < c.n_out; ++k) out[c.out_global[k]] = tmp[k];
+  }
+  return VD_OK;
+}
+
+int vd_plan_destroy(vd_plan* pl) {
+  if (!pl) return VD_OK;
+  {
+    DeviceGuard guard(pl->eng->device);
+    cudaStreamSynchronize(pl->eng->stream);
+    if (pl->graph) cudaGraphExecDestroy(pl->graph);
+  }
+  delete pl;
+  return VD_OK;
+}
+
+// ---- reference-shaped entry points --------------------------------------------------
+
+namespace {
+
+// Pack pointer-array inputs (the reference's ctypes calling convention) into a
+// vd_batch of explicit pairs; identical (pointer, length) reads and
+// haplotypes are stored once.
+struct PackedPairs {
+  std::vector<unsigned char> rb, rq, hb;
+  std::vector<int64_t> roff{0}, hoff{0};
+  std::vector<int32_t> pr, ph;
+  vd_batch batch{};
+};
+
+struct PtrKey {
+  const void* a;
+  const void* b;
+  int n;
+  bool operator==(const PtrKey& o) const { return a == o.a && b == o.b && n == o.n; }
+};
+struct PtrHash {
+  size_t operator()(const PtrKey& k) const {
+    return std::hash<const void*>()(k.a) * 31 + std::hash<const void*>()(k.b) * 7 + (size_t)k.n;
+  }
+};
+
+void pack_pairs(const char* const* reads, const unsigned char* const* quals, const int* rn,
+                const char* const* haps, const int* hn, int count, PackedPairs& pp) {
+  std::unordered_map<PtrKey, int32_t, PtrHash> rid, hid;
+  pp.pr.resize(count);
+  pp.ph.resize(count);
+  for (int p = 0; p < count; ++p) {
+    const int n = std::max(0, rn[p]);
+    PtrKey rk{reads[p], quals[p], n};
+    auto it = rid.find(rk);
+    if (it == rid.end()) {
+      const int32_t id = (int32_t)pp.roff.size() - 1;
+      pp.rb.insert(pp.rb.end(), (const unsigned char*)reads[p], (const unsigned char*)reads[p] + n);
+      pp.rq.insert(pp.rq.end(), quals[p], quals[p] + n);
+      pp.roff.push_back((int64_t)pp.rb.size());
+      it = rid.emplace(rk, id).first;
+    }
+    pp.pr[p] = it->second;
+    const int m = std::max(0, hn[p]);
+    PtrKey hk{haps[p], nullptr, m};
+    auto jt = hid.find(hk);
+    if (jt == hid.end()) {
+      const int32_t id = (int32_t)pp.hoff.size() - 1;
+      pp.hb.insert(pp.hb.end(), (const unsigned char*)haps[p], (const unsigned char*)haps[p] + m);
+      pp.hoff.push_back((int64_t)pp.hb.size());
+      jt = hid.emplace(hk, id).first;
+    }
+    pp.ph[p] = jt->second;
+  }
+  vd_batch& b = pp.batch;
+  b.read_bases = pp.rb.data();
+  b.read_quals = pp.rq.data();
+  b.read_off = pp.roff.data();
+  b.n_reads = (int64_t)pp.roff.size() - 1;
+  b.hap_bases = pp.hb.data();
+  b.hap_off = pp.hoff.data();
+  b.n_haps = (int64_t)pp.hoff.size() - 1;
+  b.pair_read = pp.pr.data();
+  b.pair_hap = pp.ph.data();
+  b.n_pairs = count;
+}
+
+vd_params fixed_params(int mode) {
+  vd_params p{};
+  p.gap = 0.001;
+  p.ext = 0.1;
+  p.anchored = mode == 1 ? 1 : 0;
+  p.precision = default_precision();
+  return p;
+}
+
+double single_pair(const char* read, const unsigned char* qual, int n, const char* hap, int m, double gap,
+                   double ext, int anchored) {
+  if (n <= 0 || m <= 0) return -HUGE_VAL;
+  vd_engine* e = nullptr;
+  if (default_engine(&e)) return NAN;
+  int64_t roff[2] = {0, n}, hoff[2] = {0, m}, rr[2] = {0, 1}, hr[2] = {0, 1};
+  vd_batch b{};
+  b.read_bases = (const unsigned char*)read;
+  b.read_quals = qual;
+  b.read_off = roff;
+  b.n_reads = 1;
+  b.hap_bases = (const unsigned char*)hap;
+  b.hap_off = hoff;
+  b.n_haps = 1;
+  b.region_read_off = rr;
+  b.region_hap_off = hr;
+  b.n_regions = 1;
+  vd_params p{};
+  p.gap = gap;
+  p.ext = ext;
+  p.anchored = anchored;
+  p.precision = default_precision();
+  double out = NAN;
+  if (vd_forward(e, &b, &p, &out, nullptr)) return NAN;
+  return out;
+}
+
+}  // namespace
+
+int vd_pairhmm_pairs(const char* const* reads, const unsigned char* const* quals, const int* rn,
+                     const char* const* haps, const int* hn, int count, int mode, int lanes, double* out) {
+  (void)lanes;
+  if (count < 0 || mode < 0 || mode > 2) return fail(VD_EINVAL, "count < 0 or mode outside 0..2");
+  if (count == 0) return VD_OK;
+  if (!reads || !quals || !rn || !haps || !hn || !out) return fail(VD_EINVAL, "NULL argument");
+  vd_engine* e = nullptr;
+  int rc = default_engine(&e);
+  if (rc) return rc;
+  PackedPairs pp;
+  pack_pairs(reads, quals, rn, haps, hn, count, pp);
+  vd_params p = fixed_params(mode);
+  return vd_forward(e, &pp.batch, &p, out, nullptr);
+}
+
+int vd_trie_many(const char* const* reads, const unsigned char* const* quals, const int* rn, int nr,
+                 const char* const* haps, const int* hn, int nh, int mode, int lanes, double* out,
+                 uint64_t* cells) {
+  (void)lanes;
+  if (nr < 0 || nh < 0 || mode < 0 || mode > 2) return fail(VD_EINVAL, "nr/nh < 0 or mode outside 0..2");
+  if (cells) *cells = 0;
+  if (nr == 0 || nh == 0) return VD_OK;
+  if (!reads || !quals || !rn || !haps || !hn || !out) return fail(VD_EINVAL, "NULL argument");
+  vd_engine* e = nullptr;
+  int rc = default_engine(&e);
+  if (rc) return rc;
+  std::vector<unsigned char> rb, rq, hb;
+  std::vector<int64_t> roff{0}, hoff{0};
+  for (int r = 0; r < nr; ++r) {
+    const int n = std::max(0, rn[r]);
+    rb.insert(rb.end(), (const unsigned char*)reads[r], (const unsigned char*)reads[r] + n);
+    rq.insert(rq.end(), quals[r], quals[r] + n);
+    roff.push_back((int64_t)rb.size());
+  }
+  for (int h = 0; h < nh; ++h) {
+    const int m = std::max(0, hn[h]);
+    hb.insert(hb.end(), (const unsigned char*)haps[h], (const unsigned char*)haps[h] + m);
+    hoff.push_back((int64_t)hb.size());
+  }
+  int64_t rr[2] = {0, nr}, hr[2] = {0, nh};
+  vd_batch b{};
+  b.read_bases = rb.data();
+  b.read_quals = rq.data();
+  b.read_off = roff.data();
+  b.n_reads = nr;
+  b.hap_bases = hb.data();
+  b.hap_off = hoff.data();
+  b.n_haps = nh;
+  b.region_read_off = rr;
+  b.region_hap_off = hr;
+  b.n_regions = 1;
+  vd_params p = fixed_params(mode);
+  vd_stats s{};
+  rc = vd_forward(e, &b, &p, out, &s);
+  if (!rc && cells) *cells = (uint64_t)s.dp_cells;
+  return rc;
+}
+
+int vd_read_haplotype_batch_mode(const char* read, const unsigned char* qual, int n, const char* const* haps,
+                                 const int* lengths, int count, double gap, double ext, double* out, int mode) {
+  (void)mode;
+  if (count < 0) return fail(VD_EINVAL, "count < 0");
+  if (count == 0) return VD_OK;
+  if (!haps || !lengths || !out || (n > 0 && (!read || !qual))) return fail(VD_EINVAL, "NULL argument");
+  vd_engine* e = nullptr;
+  int rc = default_engine(&e);
+  if (rc) return rc;
+  std::vector<unsigned char> hb;
+  std::vector<int64_t> hoff{0};
+  for (int h = 0; h < count; ++h) {
+    const int m = std::max(0, lengths[h]);
+    hb.insert(hb.end(), (const unsigned char*)haps[h], (const unsigned char*)haps[h] + m);
+    hoff.push_back((int64_t)hb.size());
+  }
+  int64_t roff[2] = {0, std::max(0, n)}, rr[2] = {0, 1}, hr[2] = {0, count};
+  vd_batch b{};
+  b.read_bases = (const unsigned char*)read;
+  b.read_quals = qual;
+  b.read_off = roff;
+  b.n_reads = 1;
+  b.hap_bases = hb.data();
+  b.hap_off = hoff.data();
+  b.n_haps = count;
+  b.region_read_off = rr;
+  b.region_hap_off = hr;
+  b.n_regions = 1;
+  vd_params p{};
+  p.gap = gap;
+  p.ext = ext;
+  p.precision = default_precision();
+  return vd_forward(e, &b, &p, out, nullptr);
+}
+
+double vd_read_haplotype(const char* read, const unsigned char* qual, int n, const char* hap, int m, double gap,
+                         double ext) {
+  return single_pair(read, qual, n, hap, m, gap, ext, 0);
+}
+
+double vd_anchored_pairhmm(const char* read, const unsigned char* qual, int n, const char* hap, int m, double gap,
+                           double ext) {
+  return single_pair(read, qual, n, hap, m, gap, ext, 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,432 @@
+// Device code of the PairHMM wavefront.  Included once per (type, mode)
+// instantiation unit; see pairhmm_core.cuh for the model and the scaling.
+#pragma once
+#include <climits>
+#include <cmath>
+#include "pairhmm_core.cuh"
+
+namespace vd {
+
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float maxT(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double maxT(double a, double b) { return fmax(a, b); }
+
+// v *= f when the read base a differs from the haplotype base b: one compare
+// and one predicated multiply (a match leaves v untouched).
+__device__ __forceinline__ void mul_if_ne(float& v, uint32_t a, uint32_t b, float f) {
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, %2;\n\t@p mul.rn.f32 %0, %0, %3;\n\t}"
+      : "+f"(v) : "r"(a), "r"(b), "f"(f));
+}
+__device__ __forceinline__ void mul_if_ne(double& v, uint32_t a, uint32_t b, double f) {
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, %2;\n\t@p mul.rn.f64 %0, %0, %3;\n\t}"
+      : "+d"(v) : "r"(a), "r"(b), "d"(f));
+}
+
+// 2^k for k inside the normal range of T.
+__device__ __forceinline__ float pow2T(int k, float) { return __int_as_float((k + 127) << 23); }
+__device__ __forceinline__ double pow2T(int k, double) {
+  return __longlong_as_double((long long)(k + 1023) << 52);
+}
+template <typename T> struct ExpLimits;
+template <> struct ExpLimits<float> { static constexpr int lo = -126, hi = 127; };
+template <> struct ExpLimits<double> { static constexpr int lo = -1022, hi = 1023; };
+
+// The R rows a lane owns: per-row constants and the state of the column the
+// lane finished last.
+template <typename T, int R, bool GEN>
+struct LaneRows {
+  uint32_t rb[R];          // read base (0 for padding rows: never equals a base)
+  T miss[R];               // mismatch factor
+  T hit[GEN ? R : 1];      // match factor (only when some row has P0 > P1)
+  T K[R], X[R];            // k1 f_i and (x/4) f_i
+  T mu[R], om[R], s[R];    // mu, omega and s of the previous column
+};
+
+// One DP column of this lane.  s_top is s of the row above at column j-1,
+// u_top is u of the row above at column j.  The row RN values are tapped for
+// the final row sums.
+template <typename T, int R, int RN, bool GEN>
+__device__ __forceinline__ void column(LaneRows<T, R, GEN>& w, uint32_t hb, T s_top, T u_top,
+                                       T k2, T x, T& u_bot, T& tap_mu, T& tap_nu, T& tap_om) {
+  T s_above = s_top;
+  T nu = u_top;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    T mu_new = s_above;
+    if (GEN) {
+      mu_new = s_above * (w.rb[r] == hb ? w.hit[r] : w.miss[r]);
+    } else {
+      mul_if_ne(mu_new, w.rb[r], hb, w.miss[r]);
+    }
+    const T om_new = fmaT(x, w.om[r], w.mu[r]);
+    const T u_new = fmaT(w.X[r], nu, mu_new);
+    const T s_new = fmaT(k2, om_new, fmaT(w.K[r], nu, mu_new));
+    if (r == RN) { tap_mu = mu_new; tap_nu = nu; tap_om = om_new; }
+    s_above = w.s[r];
+    w.mu[r] = mu_new;
+    w.om[r] = om_new;
+    w.s[r] = s_new;
+    nu = u_new;
+  }
+  u_bot = nu;
+}
+
+struct ItemRef {
+  WorkItem w;
+  bool use_sel;   // resolve haplotypes / outputs through hap_sel / out_sel
+  int tier;
+};
+
+template <typename T>
+__device__ __forceinline__ void spill_pair(const QueueView& qv, int32_t read, int64_t hap, int64_t out) {
+  if (qv.spill == nullptr) return;
+  const unsigned long long slot = atomicAdd(qv.spill_count, 1ull);
+  if ((long long)slot < qv.spill_cap) {
+    qv.spill[slot] = RescueEntry{read, (int32_t)hap, out};
+  } else {
+    atomicExch(qv.error_flag, 1);
+  }
+}
+
+constexpr int kUnroll = 8;
+
+template <typename T, int R, int RN, bool GEN, bool ANCH>
+__device__ __noinline__ void process_item(const BatchView bv, const QueueView qv, const ItemRef it,
+                                          const Tables<T>* __restrict__ tb, const Scalars<T> sc,
+                                          const int lane, typename Vec2<T>::type* __restrict__ scratch) {
+  using T2 = typename Vec2<T>::type;
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr double kLn2 = 0.6931471805599453094;
+  const WorkItem& w = it.w;
+  const int64_t roff = bv.read_off[w.read];
+  const int n = (int)(bv.read_off[w.read + 1] - roff);
+  const uint8_t* __restrict__ rbase = bv.read_bases + roff;
+  const uint8_t* __restrict__ rqual = bv.read_quals + roff;
+  const int K = w.nhap;
+  constexpr int SR = kWarp * R;
+  const int nstrips = (n + SR - 1) / SR;
+  const int last_local = (n - 1) - (nstrips - 1) * SR;
+  const int Ln = last_local / R;  // lane holding row n; RN == last_local % R
+
+  auto hap_index = [&](int k) -> int64_t {
+    return it.use_sel ? (int64_t)bv.hap_sel[w.hap_begin + k] : w.hap_begin + k;
+  };
+  auto out_index = [&](int k) -> int64_t {
+    return it.use_sel ? bv.out_sel[w.out_begin + k] : w.out_begin + k;
+  };
+
+  // sum_i ln N_i over the read (FP64), identical on every lane
+  double lnN = 0.0;
+  for (int i = lane; i < n; i += kWarp) lnN += tb->lnN[rqual[i]];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) lnN += __shfl_xor_sync(FULL, lnN, o);
+
+  const T A = tb->A[rqual[n - 1]];
+  const T k2 = sc.k2, x = sc.x, c0 = sc.c, gfin = sc.gfin;
+  int E = 0;          // total power-of-two renormalisation of the strips
+  bool fail = false;  // a strip boundary underflowed
+  T scale_in = T(1);  // factor applied to the injected boundary of this strip
+
+  for (int strip = 0; strip < nstrips; ++strip) {
+    const bool last = (strip == nstrips - 1);
+    LaneRows<T, R, GEN> rw;
+    const int row0 = strip * SR + lane * R;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = row0 + r;
+      if (i < n) {
+        const unsigned q = rqual[i];
+        rw.rb[r] = rbase[i];
+        rw.miss[r] = tb->miss[q];
+        if (GEN) rw.hit[r] = tb->hit[q];
+        rw.K[r] = tb->K[q];
+        rw.X[r] = tb->X[q];
+      } else {
+        rw.rb[r] = 0u;
+        rw.miss[r] = T(0);
+        if (GEN) rw.hit[r] = T(0);
+        rw.K[r] = T(0);
+        rw.X[r] = T(0);
+      }
+      rw.mu[r] = T(0);
+      rw.om[r] = T(0);
+      rw.s[r] = T(0);
+    }
+
+    int kL = -1;            // haplotype this lane is in
+    int next_reset = 0;     // stream position of this lane's next column 0
+    int S_cur = -1;         // stream position of this lane's current column 0
+    const uint8_t* hp = bv.hap_bases;  // hp[p] = haplotype base at stream position p
+    T s_top = T(0), u_bot = T(0);
+    T acc32 = T(0), cap = T(0), dinj = T(0), bmax = T(0);
+    double acc64 = 0.0;
+
+    auto finalize = [&](int k) {
+      const int64_t h = hap_index(k);
+      const int64_t o = out_index(k);
+      const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
+      const double Zs = ANCH ? (double)cap : acc64 + (double)acc32;
+      const double lnC0 = sc.ln_c + (ANCH ? 0.0 : log((double)(m + 1)));
+      const bool ok = !fail && Zs >= (double)sc.final_floor && Zs < HUGE_VAL;
+      if (ok || qv.spill == nullptr) {
+        bv.out[o] = (Zs > 0.0 ? log(Zs) : -HUGE_VAL) - lnC0 + lnN - (double)E * kLn2;
+      } else {
+        bv.out[o] = __longlong_as_double(0x7ff8000000000000LL);
+        spill_pair<T>(qv, w.read, h, o);
+      }
+    };
+
+    auto zero_state = [&]() {
+#pragma unroll
+      for (int r = 0; r < R; ++r) { rw.mu[r] = T(0); rw.om[r] = T(0); rw.s[r] = T(0); }
+      s_top = T(0);
+      acc32 = T(0);
+      acc64 = 0.0;
+      cap = T(0);
+    };
+
+    // the final-row tap: semiglobal sums (M + I) over every column, anchored
+    // keeps (M + I + D) of the latest column
+    auto accumulate = [&](T tmu, T tnu, T tom) {
+      if (ANCH) cap = fmaT(gfin, tom, fmaT(A, tnu, tmu));
+      else acc32 += fmaT(A, tnu, tmu);
+    };
+
+    // step with per-lane haplotype bookkeeping (ramps and short haplotypes)
+    auto gstep = [&](int t) {
+      const int p = t - lane;
+      T u_in = __shfl_up_sync(FULL, u_bot, 1);
+      T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
+      if (p == next_reset) {
+        if (last && kL >= 0 && lane == Ln) finalize(kL);
+        ++kL;
+        zero_state();
+        S_cur = p;
+        if (kL < K) {
+          const int64_t h = hap_index(kL);
+          const int64_t ho = bv.hap_off[h];
+          const int m = (int)(bv.hap_off[h + 1] - ho);
+          hp = bv.hap_bases + ho - 1 - p;
+          next_reset = p + m + 1;
+        } else {
+          next_reset = INT_MAX;
+        }
+      }
+      const bool active = kL >= 0 && kL < K;
+      const bool col0 = p == S_cur;
+      const uint32_t hb = (active && !col0) ? (uint32_t)hp[p] : 0u;
+      T iu, is;
+      if (strip == 0) {
+        if (ANCH) {
+          if (col0) { iu = c0; is = c0; dinj = k2 * c0; }
+          else { iu = T(0); is = dinj; dinj *= x; }
+        } else {
+          iu = c0; is = c0;
+        }
+      } else {
+        T2 rec = {T(0), T(0)};
+        if (lane == 0 && active) rec = scratch[p];
+        iu = rec.y * scale_in;
+        is = rec.x * scale_in;
+      }
+      if (lane == 0) { u_in = iu; s_in = is; }
+      T tmu = T(0), tnu = T(0), tom = T(0);
+      column<T, R, RN, GEN>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
+      s_top = s_in;
+      if (last) {
+        accumulate(tmu, tnu, tom);
+        if (!ANCH) { acc64 += (double)acc32; acc32 = T(0); }
+      } else {
+        if (lane == kWarp - 1 && active) {
+          scratch[p] = T2{rw.s[R - 1], u_bot};
+          bmax = maxT(bmax, maxT(rw.s[R - 1], u_bot));
+        }
+        __syncwarp();
+      }
+    };
+
+    // step with every lane inside the same haplotype at a column >= 1
+    auto sstep = [&](uint32_t hb, int p) {
+      T u_in = __shfl_up_sync(FULL, u_bot, 1);
+      T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
+      T iu, is;
+      if (strip == 0) {
+        if (ANCH) { iu = T(0); is = dinj; dinj *= x; }
+        else { iu = c0; is = c0; }
+      } else {
+        T2 rec = {T(0), T(0)};
+        if (lane == 0) rec = scratch[p];
+        iu = rec.y * scale_in;
+        is = rec.x * scale_in;
+      }
+      if (lane == 0) { u_in = iu; s_in = is; }
+      T tmu = T(0), tnu = T(0), tom = T(0);
+      column<T, R, RN, GEN>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
+      s_top = s_in;
+      if (last) {
+        accumulate(tmu, tnu, tom);
+      } else if (lane == kWarp - 1) {
+        scratch[p] = T2{rw.s[R - 1], u_bot};
+        bmax = maxT(bmax, maxT(rw.s[R - 1], u_bot));
+      }
+    };
+
+    int t = 0;
+    int S = 0;
+    for (int k = 0; k <= K; ++k) {
+      int mk = 0;
+      if (k < K) {
+        const int64_t h = hap_index(k);
+        mk = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
+      }
+      const int Snext = S + mk + 1;
+      const int gen_end = (k < K) ? min(S + kWarp, Snext) : S + kWarp;
+      for (; t < gen_end; ++t) gstep(t);
+      if (k < K) {
+        // all lanes are inside haplotype k for t in [S + 32, Snext)
+        for (; t + kUnroll <= Snext; t += kUnroll) {
+          const uint8_t* q = hp + (t - lane);
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) sstep((uint32_t)q[u], t - lane + u);
+          if (last && !ANCH) { acc64 += (double)acc32; acc32 = T(0); }
+          if (!last) __syncwarp();
+        }
+        for (; t < Snext; ++t) {
+          sstep((uint32_t)hp[t - lane], t - lane);
+          if (last && !ANCH) { acc64 += (double)acc32; acc32 = T(0); }
+        }
+      }
+      S = Snext;
+    }
+
+    if (!last) {
+      // renormalise the boundary the next strip starts from
+      __syncwarp();
+      const T bm = __shfl_sync(FULL, bmax, kWarp - 1);
+      if (!(bm >= sc.strip_floor) || !(bm < T(HUGE_VAL))) {
+        fail = true;
+        break;
+      }
+      int e = ilogb(bm);
+      int ks = sc.target_log2 - e;
+      ks = max(ExpLimits<T>::lo, min(ExpLimits<T>::hi, ks));
+      scale_in = pow2T(ks, T(0));
+      E += ks;
+    }
+  }
+
+  if (fail) {
+    // a strip underflowed: every pair of this item goes to the next tier
+    if (lane == 0) {
+      for (int k = 0; k < K; ++k) {
+        const int64_t h = hap_index(k);
+        const int64_t o = out_index(k);
+        if (qv.spill != nullptr) {
+          bv.out[o] = __longlong_as_double(0x7ff8000000000000LL);
+          spill_pair<T>(qv, w.read, h, o);
+        } else {
+          bv.out[o] = -HUGE_VAL;
+        }
+      }
+    }
+  }
+  __syncwarp();
+}
+
+template <typename T, int R, bool ANCH>
+__device__ __forceinline__ void dispatch_rn(int RN, bool gen, const BatchView& bv, const QueueView& qv,
+                                            const ItemRef& it, const Tables<T>* tb, const Scalars<T>& sc,
+                                            int lane, typename Vec2<T>::type* scratch) {
+#define VD_CASE(rn)                                                                        \
+  case rn:                                                                                 \
+    if constexpr ((rn) < R) {                                                              \
+      if (gen) process_item<T, R, (rn), true, ANCH>(bv, qv, it, tb, sc, lane, scratch);    \
+      else process_item<T, R, (rn), false, ANCH>(bv, qv, it, tb, sc, lane, scratch);       \
+    }                                                                                      \
+    break;
+  switch (RN) {
+    VD_CASE(0) VD_CASE(1) VD_CASE(2) VD_CASE(3) VD_CASE(4) VD_CASE(5) VD_CASE(6) VD_CASE(7)
+    default: break;
+  }
+#undef VD_CASE
+}
+
+template <typename T, bool ANCH>
+__device__ __forceinline__ void dispatch(int code, const BatchView& bv, const QueueView& qv,
+                                         const ItemRef& it, const Tables<T>* tb, const Scalars<T>& sc,
+                                         int lane, typename Vec2<T>::type* scratch) {
+  const int R = code_R(code), RN = code_RN(code);
+  const bool gen = code_general(code);
+  switch (R) {
+    case 1: dispatch_rn<T, 1, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 2: dispatch_rn<T, 2, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 3: dispatch_rn<T, 3, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 4: dispatch_rn<T, 4, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 5: dispatch_rn<T, 5, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 6: dispatch_rn<T, 6, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 7: dispatch_rn<T, 7, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    case 8: dispatch_rn<T, 8, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+    default: break;
+  }
+}
+
+// Persistent kernel: every warp pulls work from qv.head until the list is
+// exhausted.  tier 0 reads WorkItems; tiers 1 and 2 read the rescue list the
+// previous tier spilled (one haplotype per entry).  Tier 2 runs R = 1 (strips
+// of 32 rows, renormalised between strips), which no input can underflow.
+template <typename T, bool ANCH>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp)
+pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restrict__ gtab,
+               const Scalars<T> sc, const int tier) {
+  __shared__ Tables<T> tab;
+  {
+    const int words = (int)(sizeof(Tables<T>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(gtab);
+    int* dst = reinterpret_cast<int*>(&tab);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  using T2 = typename Vec2<T>::type;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  T2* scratch = reinterpret_cast<T2*>(qv.scratch) + gw * qv.scratch_stride;
+  // primary tier: n_items work items; rescue tiers: the count the previous
+  // tier spilled, bounded by the capacity of its list (n_items)
+  long long total = qv.n_items;
+  if (qv.items == nullptr) {
+    const long long c = (long long)*qv.count;
+    total = c < total ? c : total;
+  }
+  for (;;) {
+    unsigned long long i = 0;
+    if (lane == 0) i = atomicAdd(qv.head, 1ull);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if ((long long)i >= total) break;
+    ItemRef it;
+    it.tier = tier;
+    int code;
+    if (qv.items != nullptr) {
+      it.w = qv.items[i];
+      it.use_sel = bv.hap_sel != nullptr;
+      code = it.w.code;
+    } else {
+      const RescueEntry e = qv.entries[i];
+      it.w.read = e.read;
+      it.w.nhap = 1;
+      it.w.hap_begin = e.hap;
+      it.w.out_begin = e.out;
+      it.use_sel = false;
+      const int rc = bv.read_code[e.read];
+      code = (tier >= 2) ? make_code(1, 0, code_general(rc), true) : rc;
+      it.w.code = code;
+    }
+    dispatch<T, ANCH>(code, bv, qv, it, &tab, sc, lane, scratch);
+  }
+}
+
+}  // namespace vd

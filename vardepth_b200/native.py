@@ -1,0 +1,269 @@
+"""ctypes bindings of libvardepth_pairhmm.so (include/vardepth_pairhmm.h).
+
+The library is the only compute path: there is no CPU fallback.  Loading
+fails with an ImportError-style RuntimeError when the shared library has not
+been built, and engine creation raises RuntimeError when no CUDA device is
+usable, mirroring caller/native/caller/accelerator.py:91-96.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libvardepth_pairhmm.so"
+
+VD_OK, VD_EINVAL, VD_ECUDA, VD_ENODEV, VD_ENOMEM, VD_EOVERFLOW = range(6)
+VD_PRECISION_MIXED, VD_PRECISION_FLOAT64 = 0, 1
+
+c_i64 = ctypes.c_int64
+c_i32 = ctypes.c_int32
+c_u8p = ctypes.POINTER(ctypes.c_ubyte)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class VdParams(ctypes.Structure):
+    _fields_ = [("gap", ctypes.c_double), ("ext", ctypes.c_double), ("anchored", ctypes.c_int),
+                ("precision", ctypes.c_int), ("quality_offsets", c_dp), ("reserved", ctypes.c_int * 4)]
+
+
+class VdBatch(ctypes.Structure):
+    _fields_ = [("read_bases", c_u8p), ("read_quals", c_u8p), ("read_off", c_i64p), ("n_reads", c_i64),
+                ("hap_bases", c_u8p), ("hap_off", c_i64p), ("n_haps", c_i64),
+                ("region_read_off", c_i64p), ("region_hap_off", c_i64p), ("n_regions", c_i64),
+                ("pair_read", c_i32p), ("pair_hap", c_i32p), ("n_pairs", c_i64)]
+
+
+class VdStats(ctypes.Structure):
+    _fields_ = [("pairs", c_i64), ("dp_cells", c_i64), ("work_items", c_i64), ("batches", c_i64),
+                ("rescued_fp64", c_i64), ("rescued_robust", c_i64), ("h2d_bytes", c_i64), ("d2h_bytes", c_i64),
+                ("kernel_launches", c_i64), ("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("host_ms", ctypes.c_double), ("live_bytes", c_i64), ("primary_ms", ctypes.c_double),
+                ("rescue_ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# Every symbol include/vardepth_pairhmm.h declares, with its ctypes signature.
+SIGNATURES = {
+    "vd_engine_create": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.POINTER(ctypes.c_void_p)]),
+    "vd_engine_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "vd_engine_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "vd_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams), c_dp,
+                                  ctypes.POINTER(VdStats)]),
+    "vd_batch_outputs": (c_i64, [ctypes.POINTER(VdBatch)]),
+    "vd_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams),
+                                      ctypes.POINTER(ctypes.c_void_p)]),
+    "vd_plan_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdStats)]),
+    "vd_plan_fetch": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
+    "vd_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "vd_pairhmm_pairs": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(c_u8p),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_char_p),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp]),
+    "vd_trie_many": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(c_u8p),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp,
+                                    ctypes.POINTER(ctypes.c_uint64)]),
+    "vd_read_haplotype_batch_mode": (ctypes.c_int, [ctypes.c_char_p, c_u8p, ctypes.c_int,
+                                                    ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int),
+                                                    ctypes.c_int, ctypes.c_double, ctypes.c_double, c_dp,
+                                                    ctypes.c_int]),
+    "vd_read_haplotype": (ctypes.c_double, [ctypes.c_char_p, c_u8p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_double]),
+    "vd_anchored_pairhmm": (ctypes.c_double, [ctypes.c_char_p, c_u8p, ctypes.c_int, ctypes.c_char_p,
+                                              ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+    "vd_last_error": (ctypes.c_char_p, []),
+    "vd_device_count": (ctypes.c_int, []),
+    "vd_version": (ctypes.c_char_p, []),
+    "vd_measure_fp32_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+}
+
+_LIB = None
+_LOCK = threading.Lock()
+
+
+def library() -> ctypes.CDLL:
+    """Load the shared library (built by vardepth_b200.build) exactly once."""
+    global _LIB
+    with _LOCK:
+        if _LIB is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH.name} is not built: run `python -m vardepth_b200.build` "
+                    "(the PairHMM has no CPU fallback)")
+            lib = ctypes.CDLL(str(LIB_PATH))
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _LIB = lib
+        return _LIB
+
+
+def last_error() -> str:
+    msg = library().vd_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int, what: str) -> None:
+    if rc == VD_OK:
+        return
+    msg = f"{what} failed ({rc}): {last_error()}"
+    if rc == VD_EINVAL:
+        raise ValueError(msg)
+    if rc == VD_ENOMEM and "budget" in msg:
+        raise ValueError(msg)
+    raise RuntimeError(msg)
+
+
+def _ptr(a: np.ndarray | None, ctype):
+    if a is None:
+        return ctypes.cast(None, ctypes.POINTER(ctype))
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class Packed:
+    """Reads and haplotypes in the packed layout of vd_batch.
+
+    Holds references to every array so the pointers stay valid for the call.
+    """
+
+    def __init__(self, read_bases, read_quals, read_off, hap_bases, hap_off, *,
+                 region_read_off=None, region_hap_off=None, pair_read=None, pair_hap=None):
+        self.read_bases = np.ascontiguousarray(read_bases, dtype=np.uint8)
+        self.read_quals = np.ascontiguousarray(read_quals, dtype=np.uint8)
+        self.read_off = np.ascontiguousarray(read_off, dtype=np.int64)
+        self.hap_bases = np.ascontiguousarray(hap_bases, dtype=np.uint8)
+        self.hap_off = np.ascontiguousarray(hap_off, dtype=np.int64)
+        self.region_read_off = None if region_read_off is None else np.ascontiguousarray(region_read_off, np.int64)
+        self.region_hap_off = None if region_hap_off is None else np.ascontiguousarray(region_hap_off, np.int64)
+        self.pair_read = None if pair_read is None else np.ascontiguousarray(pair_read, np.int32)
+        self.pair_hap = None if pair_hap is None else np.ascontiguousarray(pair_hap, np.int32)
+        if self.read_bases.shape != self.read_quals.shape:
+            raise ValueError("read bases and qualities differ in length")
+        b = VdBatch()
+        b.read_bases = _ptr(self.read_bases, ctypes.c_ubyte)
+        b.read_quals = _ptr(self.read_quals, ctypes.c_ubyte)
+        b.read_off = _ptr(self.read_off, ctypes.c_int64)
+        b.n_reads = len(self.read_off) - 1
+        b.hap_bases = _ptr(self.hap_bases, ctypes.c_ubyte)
+        b.hap_off = _ptr(self.hap_off, ctypes.c_int64)
+        b.n_haps = len(self.hap_off) - 1
+        if self.pair_read is not None:
+            b.pair_read = _ptr(self.pair_read, ctypes.c_int32)
+            b.pair_hap = _ptr(self.pair_hap, ctypes.c_int32)
+            b.n_pairs = len(self.pair_read)
+        else:
+            b.region_read_off = _ptr(self.region_read_off, ctypes.c_int64)
+            b.region_hap_off = _ptr(self.region_hap_off, ctypes.c_int64)
+            b.n_regions = len(self.region_read_off) - 1
+        self.batch = b
+
+    def n_outputs(self) -> int:
+        if self.pair_read is not None:
+            return len(self.pair_read)
+        rr = np.diff(self.region_read_off)
+        hh = np.diff(self.region_hap_off)
+        return int(np.sum(rr * hh))
+
+
+def make_params(gap: float, ext: float, anchored: bool, precision: int, quality_offsets=None):
+    p = VdParams()
+    p.gap = float(gap)
+    p.ext = float(ext)
+    p.anchored = 1 if anchored else 0
+    p.precision = int(precision)
+    keep = None
+    if quality_offsets is not None:
+        keep = np.ascontiguousarray(quality_offsets, dtype=np.float64)
+        if keep.shape != (4,):
+            raise ValueError("quality_offsets must hold 4 values")
+        p.quality_offsets = keep.ctypes.data_as(c_dp)
+    return p, keep
+
+
+class Engine:
+    """One vd_engine (device, stream, cached buffers)."""
+
+    def __init__(self, device: int = 0, memory_mb: int = 4096):
+        lib = library()
+        h = ctypes.c_void_p()
+        rc = lib.vd_engine_create(int(device), int(memory_mb), ctypes.byref(h))
+        if rc == VD_ENODEV:
+            raise RuntimeError("CUDA PairHMM requires an accessible NVIDIA GPU: " + last_error())
+        check(rc, "vd_engine_create")
+        self.handle = h
+        self.device = device
+        self.memory_mb = memory_mb
+
+    def info(self) -> dict:
+        name = ctypes.create_string_buffer(256)
+        major, minor, sms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(library().vd_engine_info(self.handle, name, 256, ctypes.byref(major), ctypes.byref(minor),
+                                       ctypes.byref(sms)), "vd_engine_info")
+        return {"gpu": name.value.decode(), "compute_capability": [major.value, minor.value], "sm_count": sms.value}
+
+    def forward(self, packed: Packed, params: VdParams, out: np.ndarray | None = None):
+        n = packed.n_outputs()
+        if out is None:
+            out = np.empty(n, np.float64)
+        stats = VdStats()
+        check(library().vd_forward(self.handle, ctypes.byref(packed.batch), ctypes.byref(params),
+                                   out.ctypes.data_as(c_dp), ctypes.byref(stats)), "vd_forward")
+        return out, stats
+
+    def plan(self, packed: Packed, params: VdParams) -> "Plan":
+        return Plan(self, packed, params)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().vd_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """A device-resident batch (vd_plan_*)."""
+
+    def __init__(self, engine: Engine, packed: Packed, params: VdParams):
+        self.engine = engine
+        self.packed = packed
+        self.n_out = packed.n_outputs()
+        h = ctypes.c_void_p()
+        check(library().vd_plan_create(engine.handle, ctypes.byref(packed.batch), ctypes.byref(params),
+                                       ctypes.byref(h)), "vd_plan_create")
+        self.handle = h
+
+    def run(self) -> VdStats:
+        st = VdStats()
+        check(library().vd_plan_run(self.handle, ctypes.byref(st)), "vd_plan_run")
+        return st
+
+    def fetch(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.n_out, np.float64)
+        check(library().vd_plan_fetch(self.handle, out.ctypes.data_as(c_dp)), "vd_plan_fetch")
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().vd_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
