@@ -55,6 +55,10 @@ int vdo_quality_bin(unsigned q) {
     return 3;
 }
 
+double vdo_forward_ld_ex(const unsigned char *read, const unsigned char *qual, int n,
+                         const unsigned char *hap, int m, double gap, double ext,
+                         int anchored, int clamp);
+
 static double error_offset(unsigned q, const double *offsets) {
     if (!offsets) return error_of(q);
     double c = (double)(q < 60u ? q : 60u) + offsets[vdo_quality_bin(q)];
@@ -120,11 +124,12 @@ double vdo_forward(const unsigned char *read, const unsigned char *qual, int n,
 }
 
 /* Extended-precision variant (x87 long double, 64-bit mantissa, exponent
- * range to 2^-16382): no rescaling is needed for any read the tests use, so
- * it is an independent check on the rescaled FP64 arithmetic. */
-double vdo_forward_ld(const unsigned char *read, const unsigned char *qual, int n,
-                      const unsigned char *hap, int m, double gap, double ext,
-                      int anchored) {
+ * range to 2^-16382), renormalised only by exact powers of two: an
+ * independent check on the rescaled FP64 arithmetic, free of its underflow.
+ * clamp = 1 applies the reference's anchored 1e-300 floor (see below). */
+double vdo_forward_ld_ex(const unsigned char *read, const unsigned char *qual, int n,
+                         const unsigned char *hap, int m, double gap, double ext,
+                         int anchored, int clamp) {
     if (n <= 0 || m <= 0) return -INFINITY;
     size_t w = (size_t)m + 1;
     long double *buf = (long double *)calloc(6 * w, sizeof(long double));
@@ -173,9 +178,21 @@ double vdo_forward_ld(const unsigned char *read, const unsigned char *qual, int 
     long double z = 0.0L;
     if (anchored) z = pm[m] + pi[m] + pd[m];
     else for (int j = 0; j <= m; ++j) z += pm[j] + pi[j];
+    /* the reference's ln(max(1e-300, Z / S_n)) + ln S_n for the anchored end
+     * cell (anchored.cpp:24), with S_n the last row's maximum */
+    if (anchored && clamp) {
+        long double top = 0.0L;
+        for (int j = 0; j <= m; ++j) { long double v = pm[j] + pi[j] + pd[j]; if (v > top) top = v; }
+        if (z < 1e-300L * top) z = 1e-300L * top;
+    }
     free(buf);
     if (!(z > 0.0L)) return -INFINITY;
     return (double)(logl(z) + log_scale);
+}
+
+double vdo_forward_ld(const unsigned char *read, const unsigned char *qual, int n,
+                      const unsigned char *hap, int m, double gap, double ext, int anchored) {
+    return vdo_forward_ld_ex(read, qual, n, hap, m, gap, ext, anchored, 1);
 }
 
 /* Batch over explicit (read, haplotype) pairs held in packed buffers:

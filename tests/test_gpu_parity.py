@@ -134,16 +134,49 @@ def _argmax_agree(w, got, want):
     return agree, total
 
 
-@pytest.mark.parametrize("anchored", [False, True])
-def test_config1_sample_against_oracle(mixed, anchored):
+def test_config1_sample_against_oracle(mixed):
     w = S.config1(n_regions=24)
-    got = _with(mixed, w.gap, w.ext).score_packed(_packed(w), anchored)
-    want = _oracle_workload(w, anchored)
+    got = _with(mixed, w.gap, w.ext).score_packed(_packed(w))
+    want = _oracle_workload(w)
     err = assert_mixed_close(got, want)
     agree, total = _argmax_agree(w, got, want)
     assert agree == total
-    print(f"config1 sample anchored={anchored}: pairs {len(got)} max|dlog10| {err.max():.2e} "
+    print(f"config1 sample: pairs {len(got)} max|dlog10| {err.max():.2e} "
           f"p99 {np.quantile(err, .99):.2e} rescued {mixed.last['float64_fallback_pairs']}")
+
+
+def anchored_windows(seed, n_sites=40, reads_per_site=24):
+    """Anchored refinement jobs as indel_refine.py builds them (caller/native/caller/indel_refine.py:143-151):
+    a read span against left + allele + right haplotype windows of about the same length."""
+    rng = np.random.default_rng(seed)
+    pairs = []
+    for _ in range(n_sites):
+        ref = "".join(rng.choice(list("ACGT"), 400))
+        p = int(rng.integers(150, 250))
+        k = int(rng.integers(1, 11))
+        alt = ref[:p] + ref[p + k:] if rng.random() < 0.5 else ref[:p] + "".join(rng.choice(list("ACGT"), k)) + ref[p:]
+        for _ in range(reads_per_site):
+            src = alt if rng.random() < 0.5 else ref
+            a = int(rng.integers(20, 120))
+            b = int(rng.integers(p + 20, min(len(src), p + 140)))
+            read = list(src[a:b])
+            for i in np.flatnonzero(rng.random(len(read)) < 0.01):
+                read[i] = "ACGT"[("ACGT".index(read[i]) + int(rng.integers(1, 4))) % 4]
+            q = rng.choice([10, 20, 30, 40], len(read), p=[.05, .15, .5, .3])
+            for hap in (ref, alt):
+                w0 = a
+                w1 = b + (len(hap) - len(src))
+                pairs.append(("".join(read), q, hap[w0:w1]))
+    return pairs
+
+
+def test_anchored_refinement_windows(mixed, fp64):
+    pairs = anchored_windows(5)
+    want = np.array([O.forward(s, q.astype(np.uint8), h, 0.001, 0.1, True, 0) for s, q, h in pairs])
+    np.testing.assert_allclose(_with(fp64, 0.001, 0.1).score(pairs, True), want, atol=FP64_ATOL_LN, rtol=0)
+    err = assert_mixed_close(_with(mixed, 0.001, 0.1).score(pairs, True), want)
+    print(f"anchored windows: pairs {len(pairs)} max|dlog10| {err.max():.2e} "
+          f"rescued {mixed.last['float64_fallback_pairs']}")
 
 
 def test_config2_precision_stress(mixed):
@@ -176,7 +209,7 @@ def test_long_reads_strip_mined(mixed, fp64, anchored):
 
 
 def test_pairs_regions_and_chunking_agree():
-    w = S.config1(n_regions=12)
+    w = S.config1(n_regions=200)
     eng = CudaPairHMM(memory_mb=4096, gap=w.gap, ext=w.ext)
     regions = eng.score_packed(_packed(w))
     pr, ph = w.explicit_pairs()
@@ -223,7 +256,7 @@ def test_reference_shaped_entry_points():
         out = np.empty(count)
         rc = lib.vd_pairhmm_pairs(reads, ctypes.cast(quals, ctypes.POINTER(native.c_u8p)), rn, haps, hn, count, mode,
                                   8, out.ctypes.data_as(native.c_dp))
-        assert rc == 0
+        assert rc == 0, native.last_error()
         assert_mixed_close(out, d[key])
     # trie_many: reads x haplotypes of config0 at the production constants
     g = golden("config0_q30")

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -38,6 +39,9 @@ int fail(int code, const std::string& msg) {
 }
 
 int cuda_fail(cudaError_t e, const char* what) {
+  // consume the thread's last-error slot so a later launch check does not
+  // report this (non-sticky) error again
+  cudaGetLastError();
   return fail(VD_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -156,6 +160,8 @@ struct vd_engine {
   // batch arena reused by vd_forward
   DevBuf arena;
   std::vector<double> out_stage;
+  // live plans: destroying the engine first releases their device resources
+  std::unordered_set<vd_plan*> plans;
 };
 
 namespace {
@@ -269,22 +275,46 @@ struct HostChunk {
 // could not resolve, and its strip scratch then stays small.
 constexpr int kRobustBlocks = 32;
 
-// Sort items by decreasing cost so that the persistent warps finish together
-// (longest-processing-time first), with an O(n) bucket pass.
+// Order the work list for the persistent warps.  Items are grouped by kernel
+// variant (the code: rows per lane, final-row register, emission form) so that
+// the warps resident on an SM run the same unrolled loop at the same time --
+// interleaving variants thrashes the instruction cache -- and inside a group
+// they run longest-processing-time first.  Groups with the largest items come
+// first, so the tail of the whole list holds the smallest items.  O(n) passes.
 void order_items(std::vector<WorkItem>& items, const std::vector<int64_t>& cost) {
+  const size_t n = items.size();
+  if (n < 2) return;
+  // cost bucket (descending) inside a group
   const int nb = 256;
-  std::vector<int64_t> count(nb + 1, 0);
-  std::vector<int> key(items.size());
-  for (size_t i = 0; i < items.size(); ++i) {
+  std::vector<int> bucket(n);
+  for (size_t i = 0; i < n; ++i) {
     const double c = (double)std::max<int64_t>(1, cost[i]);
     int k = (int)(std::log2(c) * 4.0);
     k = std::max(0, std::min(nb - 1, k));
-    key[i] = nb - 1 - k;  // descending
+    bucket[i] = nb - 1 - k;
+  }
+  // groups ordered by decreasing mean cost
+  std::unordered_map<int32_t, std::pair<double, int64_t>> stat;
+  for (size_t i = 0; i < n; ++i) {
+    auto& st = stat[items[i].code];
+    st.first += (double)cost[i];
+    st.second += 1;
+  }
+  std::vector<std::pair<double, int32_t>> groups;
+  for (auto& kv : stat) groups.push_back({kv.second.first / (double)kv.second.second, kv.first});
+  std::sort(groups.begin(), groups.end(), [](auto& a, auto& b) { return a.first > b.first || (a.first == b.first && a.second < b.second); });
+  std::unordered_map<int32_t, int> rank;
+  for (size_t g = 0; g < groups.size(); ++g) rank[groups[g].second] = (int)g;
+  const int ng = (int)groups.size();
+  std::vector<int64_t> count((size_t)ng * nb + 1, 0);
+  std::vector<int64_t> key(n);
+  for (size_t i = 0; i < n; ++i) {
+    key[i] = (int64_t)rank[items[i].code] * nb + bucket[i];
     ++count[key[i] + 1];
   }
-  for (int k = 0; k < nb; ++k) count[k + 1] += count[k];
-  std::vector<WorkItem> out(items.size());
-  for (size_t i = 0; i < items.size(); ++i) out[count[key[i]]++] = items[i];
+  for (size_t k = 0; k + 1 < count.size(); ++k) count[k + 1] += count[k];
+  std::vector<WorkItem> out(n);
+  for (size_t i = 0; i < n; ++i) out[count[key[i]]++] = items[i];
   items.swap(out);
 }
 
@@ -574,18 +604,24 @@ int upload_chunk(vd_plan* pl, const vd_batch* b, int64_t* h2d) {
 
 // Enqueue the three tiers on the engine stream, bracketed by the engine's
 // events: ev_begin .. ev_mid is the primary tier, ev_mid .. ev_end the rescue.
-int enqueue_tiers(vd_plan* pl, int* launches) {
+int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   vd_engine* e = pl->eng;
   char* d = pl->base;
   const Layout& L = pl->L;
   const bool anch = pl->params.anchored != 0;
   const bool f64 = pl->params.precision == VD_PRECISION_FLOAT64;
   unsigned long long* cnt = (unsigned long long*)(d + L.o_cnt);
+  // inside a stream capture an event becomes a graph node only when recorded
+  // as external; otherwise it would only order the capture
+  const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  cudaGetLastError();  // launch checks below must see only their own errors
   // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag
   VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), e->stream));
-  VD_CUDA(cudaEventRecord(e->ev_begin, e->stream));
+  VD_CUDA(cudaEventRecordWithFlags(e->ev_begin, e->stream, evflags));
   const BatchView bv = batch_view(pl);
+  // device tables by address; the scalars by value from the host copy
   TableSet* dt = (TableSet*)e->dtab.p;
+  const TableSet* ht = e->htab;
   QueueView q{};
   q.scratch = d + L.o_scratch;
   q.scratch_stride = L.scratch_stride;
@@ -602,11 +638,11 @@ int enqueue_tiers(vd_plan* pl, int* launches) {
   q.spill_cap = cap;
   int n = 0;
   if (!pl->chunk.items.empty()) {
-    cudaError_t err = f64 ? launch_f64(anch, bv, q, &dt->f64, dt->s64, 1, e->grid[1][anch], e->stream)
-                          : launch_f32(anch, bv, q, &dt->f32, dt->s32, 0, e->grid[0][anch], e->stream);
+    cudaError_t err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], e->stream)
+                          : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], e->stream);
     if (err != cudaSuccess) return cuda_fail(err, "primary tier launch");
     ++n;
-    VD_CUDA(cudaEventRecord(e->ev_mid, e->stream));
+    VD_CUDA(cudaEventRecordWithFlags(e->ev_mid, e->stream, evflags));
     BatchView rv = bv;
     rv.hap_sel = nullptr;
     rv.out_sel = nullptr;
@@ -620,7 +656,7 @@ int enqueue_tiers(vd_plan* pl, int* launches) {
       q1.head = cnt + 1;
       q1.spill = (RescueEntry*)(d + L.o_sp2);
       q1.spill_count = cnt + 4;
-      err = launch_f64(anch, rv, q1, &dt->f64, dt->s64, 1, e->grid[1][anch], e->stream);
+      err = launch_f64(anch, rv, q1, &dt->f64, ht->s64, 1, e->grid[1][anch], e->stream);
       if (err != cudaSuccess) return cuda_fail(err, "rescue tier launch");
       ++n;
     }
@@ -635,13 +671,13 @@ int enqueue_tiers(vd_plan* pl, int* launches) {
     q2.spill_count = nullptr;
     q2.spill_cap = 0;
     const int robust_grid = pl->chunk.any_strip ? e->grid[1][anch] : std::min(e->grid[1][anch], kRobustBlocks);
-    err = launch_f64(anch, rv, q2, &dt->f64, dt->s64, 2, robust_grid, e->stream);
+    err = launch_f64(anch, rv, q2, &dt->f64, ht->s64, 2, robust_grid, e->stream);
     if (err != cudaSuccess) return cuda_fail(err, "robust tier launch");
     ++n;
   } else {
-    VD_CUDA(cudaEventRecord(e->ev_mid, e->stream));
+    VD_CUDA(cudaEventRecordWithFlags(e->ev_mid, e->stream, evflags));
   }
-  VD_CUDA(cudaEventRecord(e->ev_end, e->stream));
+  VD_CUDA(cudaEventRecordWithFlags(e->ev_end, e->stream, evflags));
   if (launches) *launches = n;
   return VD_OK;
 }
@@ -759,6 +795,15 @@ int vd_engine_destroy(vd_engine* e) {
   {
     DeviceGuard guard(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
+    // plans still alive become empty shells; vd_plan_destroy frees the shell
+    for (vd_plan* pl : e->plans) {
+      if (pl->graph) cudaGraphExecDestroy(pl->graph);
+      pl->graph = nullptr;
+      pl->own.release();
+      pl->base = nullptr;
+      pl->eng = nullptr;
+    }
+    e->plans.clear();
     e->arena.release();
     e->dtab.release();
     if (e->htab) cudaFreeHost(e->htab);
@@ -916,12 +961,14 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
   cudaError_t err = cudaStreamSynchronize(e->stream);
   if (err != cudaSuccess) { delete pl; return cuda_fail(err, "plan upload"); }
   // the input buffers of the batch are no longer needed on the host side
+  e->plans.insert(pl);
   *out = pl;
   return VD_OK;
 }
 
 int vd_plan_run(vd_plan* pl, vd_stats* st) {
   if (!pl) return fail(VD_EINVAL, "plan is NULL");
+  if (!pl->eng) return fail(VD_EINVAL, "the plan's engine was destroyed");
   vd_engine* e = pl->eng;
   const double t0 = now_ms();
   std::lock_guard<std::mutex> lk(e->mu);
@@ -932,7 +979,7 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
   if (!pl->graph) {
     cudaGraph_t g = nullptr;
     VD_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-    rc = enqueue_tiers(pl, &launches);
+    rc = enqueue_tiers(pl, &launches, true);
     cudaError_t err = cudaStreamEndCapture(e->stream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     if (err != cudaSuccess) return cuda_fail(err, "graph capture");
@@ -970,6 +1017,7 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
 
 int vd_plan_fetch(vd_plan* pl, double* out) {
   if (!pl) return fail(VD_EINVAL, "plan is NULL");
+  if (!pl->eng) return fail(VD_EINVAL, "the plan's engine was destroyed");
   vd_engine* e = pl->eng;
   const HostChunk& c = pl->chunk;
   if (c.n_out > 0 && !out) return fail(VD_EINVAL, "out is NULL");
@@ -991,10 +1039,14 @@ int vd_plan_fetch(vd_plan* pl, double* out) {
 
 int vd_plan_destroy(vd_plan* pl) {
   if (!pl) return VD_OK;
-  {
-    DeviceGuard guard(pl->eng->device);
-    cudaStreamSynchronize(pl->eng->stream);
+  if (vd_engine* e = pl->eng) {
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard guard(e->device);
+    cudaStreamSynchronize(e->stream);
     if (pl->graph) cudaGraphExecDestroy(pl->graph);
+    pl->graph = nullptr;
+    pl->own.release();
+    e->plans.erase(pl);
   }
   delete pl;
   return VD_OK;

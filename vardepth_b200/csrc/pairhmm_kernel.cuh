@@ -32,9 +32,6 @@ __device__ __forceinline__ float pow2T(int k, float) { return __int_as_float((k 
 __device__ __forceinline__ double pow2T(int k, double) {
   return __longlong_as_double((long long)(k + 1023) << 52);
 }
-template <typename T> struct ExpLimits;
-template <> struct ExpLimits<float> { static constexpr int lo = -126, hi = 127; };
-template <> struct ExpLimits<double> { static constexpr int lo = -1022, hi = 1023; };
 
 // The R rows a lane owns: per-row constants and the state of the column the
 // lane finished last.
@@ -93,7 +90,7 @@ __device__ __forceinline__ void spill_pair(const QueueView& qv, int32_t read, in
   }
 }
 
-constexpr int kUnroll = 8;
+constexpr int kUnroll = 4;
 
 template <typename T, int R, int RN, bool GEN, bool ANCH>
 __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv, const ItemRef it,
@@ -130,7 +127,6 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   const T k2 = sc.k2, x = sc.x, c0 = sc.c, gfin = sc.gfin;
   int E = 0;          // total power-of-two renormalisation of the strips
   bool fail = false;  // a strip boundary underflowed
-  T scale_in = T(1);  // factor applied to the injected boundary of this strip
 
   for (int strip = 0; strip < nstrips; ++strip) {
     const bool last = (strip == nstrips - 1);
@@ -163,7 +159,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     int S_cur = -1;         // stream position of this lane's current column 0
     const uint8_t* hp = bv.hap_bases;  // hp[p] = haplotype base at stream position p
     T s_top = T(0), u_bot = T(0);
-    T acc32 = T(0), cap = T(0), dinj = T(0), bmax = T(0);
+    T acc32 = T(0), cap = T(0), rmax = T(0), dinj = T(0), bmax = T(0);
     double acc64 = 0.0;
 
     auto finalize = [&](int k) {
@@ -171,10 +167,14 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       const int64_t o = out_index(k);
       const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
       const double Zs = ANCH ? (double)cap : acc64 + (double)acc32;
+      // anchored.cpp:24 returns ln(max(1e-300, Z / S_n)) + ln S_n, S_n the max of
+      // (M+I+D) over the last row: the clamp binds when the end cell lies more
+      // than 1e-300 below that row maximum
+      const double Zc = ANCH ? fmax(Zs, 1e-300 * (double)rmax) : Zs;
       const double lnC0 = sc.ln_c + (ANCH ? 0.0 : log((double)(m + 1)));
       const bool ok = !fail && Zs >= (double)sc.final_floor && Zs < HUGE_VAL;
       if (ok || qv.spill == nullptr) {
-        bv.out[o] = (Zs > 0.0 ? log(Zs) : -HUGE_VAL) - lnC0 + lnN - (double)E * kLn2;
+        bv.out[o] = (Zc > 0.0 ? log(Zc) : -HUGE_VAL) - lnC0 + lnN - (double)E * kLn2;
       } else {
         bv.out[o] = __longlong_as_double(0x7ff8000000000000LL);
         spill_pair<T>(qv, w.read, h, o);
@@ -188,13 +188,18 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       acc32 = T(0);
       acc64 = 0.0;
       cap = T(0);
+      rmax = T(0);
     };
 
     // the final-row tap: semiglobal sums (M + I) over every column, anchored
     // keeps (M + I + D) of the latest column
     auto accumulate = [&](T tmu, T tnu, T tom) {
-      if (ANCH) cap = fmaT(gfin, tom, fmaT(A, tnu, tmu));
-      else acc32 += fmaT(A, tnu, tmu);
+      if (ANCH) {
+        cap = fmaT(gfin, tom, fmaT(A, tnu, tmu));
+        rmax = maxT(rmax, cap);
+      } else {
+        acc32 += fmaT(A, tnu, tmu);
+      }
     };
 
     // step with per-lane haplotype bookkeeping (ramps and short haplotypes)
@@ -231,8 +236,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       } else {
         T2 rec = {T(0), T(0)};
         if (lane == 0 && active) rec = scratch[p];
-        iu = rec.y * scale_in;
-        is = rec.x * scale_in;
+        iu = rec.y;
+        is = rec.x;
       }
       if (lane == 0) { u_in = iu; s_in = is; }
       T tmu = T(0), tnu = T(0), tom = T(0);
@@ -261,8 +266,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       } else {
         T2 rec = {T(0), T(0)};
         if (lane == 0) rec = scratch[p];
-        iu = rec.y * scale_in;
-        is = rec.x * scale_in;
+        iu = rec.y;
+        is = rec.x;
       }
       if (lane == 0) { u_in = iu; s_in = is; }
       T tmu = T(0), tnu = T(0), tom = T(0);
@@ -305,17 +310,25 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     }
 
     if (!last) {
-      // renormalise the boundary the next strip starts from
+      // renormalise the boundary the next strip starts from: its maximum is
+      // brought to 2^target by an exact power of two, applied as two factors
+      // so that any exponent shift stays representable
       __syncwarp();
       const T bm = __shfl_sync(FULL, bmax, kWarp - 1);
       if (!(bm >= sc.strip_floor) || !(bm < T(HUGE_VAL))) {
         fail = true;
         break;
       }
-      int e = ilogb(bm);
-      int ks = sc.target_log2 - e;
-      ks = max(ExpLimits<T>::lo, min(ExpLimits<T>::hi, ks));
-      scale_in = pow2T(ks, T(0));
+      const int ks = sc.target_log2 - ilogb(bm);
+      const int k1 = ks / 2;
+      const T f1 = pow2T(k1, T(0)), f2 = pow2T(ks - k1, T(0));
+      for (int p = lane; p < S - 1; p += kWarp) {
+        T2 v = scratch[p];
+        v.x = (v.x * f1) * f2;
+        v.y = (v.y * f1) * f2;
+        scratch[p] = v;
+      }
+      __syncwarp();
       E += ks;
     }
   }

@@ -202,6 +202,8 @@ class Engine:
         self.handle = h
         self.device = device
         self.memory_mb = memory_mb
+        import weakref
+        self._plans = weakref.WeakSet()
 
     def info(self) -> dict:
         name = ctypes.create_string_buffer(256)
@@ -224,6 +226,8 @@ class Engine:
 
     def close(self):
         if getattr(self, "handle", None):
+            for plan in list(self._plans):
+                plan.close()
             library().vd_engine_destroy(self.handle)
             self.handle = None
 
@@ -245,6 +249,7 @@ class Plan:
         check(library().vd_plan_create(engine.handle, ctypes.byref(packed.batch), ctypes.byref(params),
                                        ctypes.byref(h)), "vd_plan_create")
         self.handle = h
+        engine._plans.add(self)
 
     def run(self) -> VdStats:
         st = VdStats()
