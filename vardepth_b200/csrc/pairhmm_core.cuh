@@ -8,8 +8,9 @@
 //   E_ij = read[i-1]==hap[j-1] ? 1-e_i : e_i/3,  e = 10^(-min(q,60)/10)
 //
 // Work decomposition.  A warp owns one read (n rows) and streams through a list
-// of K haplotypes.  Lane L owns rows L*R+1 .. L*R+R of the current strip of
-// 32*R rows (reads longer than 256 bases are strip-mined with R = 8).  At step
+// of K haplotypes.  Lane L owns R consecutive rows of the current strip of
+// 32*R rows (reads longer than 256 bases are strip-mined with R = 8); the
+// placement of the read in the strip is described at process_item.  At step
 // t lane L is at position p = t - L of the "column stream": haplotype k
 // occupies positions S_k (its column 0) .. S_k + m_k.  Consecutive haplotypes
 // follow each other without a gap, so the 31-step wavefront ramp is paid once
@@ -46,7 +47,7 @@ struct WorkItem {
   int32_t nhap;       // haplotypes in the list
   int64_t hap_begin;  // first haplotype (contiguous lists) or offset into hap_sel
   int64_t out_begin;  // output slot of the first haplotype, or offset into out_sel
-  int32_t code;       // R | RN << 4 | general << 8 | multistrip << 9
+  int32_t code;       // R | general << 8 | multistrip << 9
   int32_t tier;       // 0 primary, 1 rescue (FP64), 2 robust (FP64, R = 1)
 };
 
@@ -58,10 +59,9 @@ struct RescueEntry {
 };
 
 inline __host__ __device__ int code_R(int c) { return c & 15; }
-inline __host__ __device__ int code_RN(int c) { return (c >> 4) & 15; }
 inline __host__ __device__ bool code_general(int c) { return (c >> 8) & 1; }
-inline __host__ __device__ int make_code(int R, int RN, bool general, bool multistrip) {
-  return R | (RN << 4) | (general ? 256 : 0) | (multistrip ? 512 : 0);
+inline __host__ __device__ int make_code(int R, bool general, bool multistrip) {
+  return R | (general ? 256 : 0) | (multistrip ? 512 : 0);
 }
 
 // Per-quality tables (index = raw Phred byte) and scalar constants for one

@@ -323,7 +323,7 @@ struct ReadInfo {
   int32_t code;
 };
 
-ReadInfo read_info(const vd_batch* b, int64_t r) {
+ReadInfo read_info(const vd_batch* b, int64_t r, bool anchored) {
   const int64_t o = b->read_off[r];
   const int n = (int)(b->read_off[r + 1] - o);
   ReadInfo ri{n, 0};
@@ -334,8 +334,9 @@ ReadInfo read_info(const vd_batch* b, int64_t r) {
     // P0 > P1 only for Phred 0 and 1 (e > 0.75); offsets can move a bin there
     if (q[i] < 2) { gen = true; break; }
   }
-  const int R = rows_per_lane(n);
-  ri.code = make_code(R, (n - 1) % R, gen, n > kStripRows);
+  // anchored reads carry one extra row on top: the emulator of row 0
+  const int rows = n + (anchored ? 1 : 0);
+  ri.code = make_code(rows_per_lane(rows), gen, rows > kStripRows);
   return ri;
 }
 
@@ -348,18 +349,19 @@ bool read_general(const vd_batch* b, int64_t r, const TableSet* ts) {
   return false;
 }
 
-void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bool offsets) {
+void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bool offsets, bool anchored) {
   c.read_off.resize(c.rb - c.ra + 1);
   c.read_code.resize(c.rb - c.ra);
   const int64_t r0 = b->read_off[c.ra];
   for (int64_t r = c.ra; r <= c.rb; ++r) c.read_off[r - c.ra] = b->read_off[r] - r0;
   for (int64_t r = c.ra; r < c.rb; ++r) {
-    ReadInfo ri = read_info(b, r);
+    ReadInfo ri = read_info(b, r, anchored);
     if (offsets && ri.n > 0 && !code_general(ri.code) && read_general(b, r, ts))
       ri.code |= 256;
     c.read_code[r - c.ra] = ri.code;
-    if (ri.n > kWarp) c.any_long = true;
-    if (ri.n > kStripRows) c.any_strip = true;
+    const int rows = ri.n + (anchored ? 1 : 0);
+    if (ri.n > 0 && rows > kWarp) c.any_long = true;
+    if (ri.n > 0 && rows > kStripRows) c.any_strip = true;
   }
   c.hap_off.resize(c.hb - c.ha + 1);
   const int64_t h0 = b->hap_off[c.ha];
@@ -372,7 +374,7 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
 // haplotypes as contiguous runs; reads longer than a strip get one item per
 // haplotype (their strip boundary scratch holds one haplotype).
 void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSet* ts, bool offsets,
-                        HostChunk& c) {
+                        bool anchored, HostChunk& c) {
   c.ra = b->region_read_off[g0];
   c.rb = b->region_read_off[g1];
   c.ha = b->region_hap_off[g0];
@@ -380,7 +382,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   c.out_begin = 0;
   for (int64_t g = 0; g < g0; ++g)
     c.out_begin += (b->region_read_off[g + 1] - b->region_read_off[g]) * (b->region_hap_off[g + 1] - b->region_hap_off[g]);
-  finish_chunk_common(c, b, ts, offsets);
+  finish_chunk_common(c, b, ts, offsets, anchored);
   std::vector<int64_t> cost;
   int64_t out = 0;
   const int kMaxStream = 1 << 30;
@@ -393,8 +395,9 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
       if (n <= 0) continue;
       const int R = code_R(code);
-      const int64_t rows = (int64_t)kWarp * R * ((n + kWarp * R - 1) / (kWarp * R));
-      const bool multistrip = n > kStripRows;
+      const int n_rows = n + (anchored ? 1 : 0);
+      const int64_t rows = (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R));
+      const bool multistrip = n_rows > kStripRows;
       int64_t h = h_lo;
       while (h < h_hi) {
         const int m0 = (int)(b->hap_off[h + 1] - b->hap_off[h]);
@@ -443,20 +446,21 @@ void group_pairs(const vd_batch* b, PairGroups& pg) {
 }
 
 void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64_t rb, const TableSet* ts,
-                      bool offsets, HostChunk& c) {
+                      bool offsets, bool anchored, HostChunk& c) {
   c.ra = ra;
   c.rb = rb;
   c.ha = 0;
   c.hb = b->n_haps;
-  finish_chunk_common(c, b, ts, offsets);
+  finish_chunk_common(c, b, ts, offsets, anchored);
   std::vector<int64_t> cost;
   const int kMaxStream = 1 << 30;
   for (int64_t r = ra; r < rb; ++r) {
     const int32_t code = c.read_code[r - ra];
     const int n = (int)(c.read_off[r - ra + 1] - c.read_off[r - ra]);
     const int R = code_R(code);
-    const bool multistrip = n > kStripRows;
-    const int64_t rows = n > 0 ? (int64_t)kWarp * R * ((n + kWarp * R - 1) / (kWarp * R)) : 0;
+    const int n_rows = n + (anchored ? 1 : 0);
+    const bool multistrip = n_rows > kStripRows;
+    const int64_t rows = n > 0 ? (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R)) : 0;
     int64_t list_begin = (int64_t)c.hap_sel.size();
     int64_t stream = 0;
     auto flush = [&]() {
@@ -870,7 +874,7 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   int64_t max_hap = 0, max_read = 0;
   for (int64_t h = 0; h < b->n_haps; ++h) max_hap = std::max<int64_t>(max_hap, b->hap_off[h + 1] - b->hap_off[h]);
   for (int64_t r = 0; r < b->n_reads; ++r) max_read = std::max<int64_t>(max_read, b->read_off[r + 1] - b->read_off[r]);
-  const int64_t scratch_warps = max_read > kStripRows ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
+  const int64_t scratch_warps = max_read + p->anchored > kStripRows ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
   fixed += (max_hap + 1) * scratch_warps * (int64_t)sizeof(double2) + 64 * 1024;
   const int64_t budget = (int64_t)e->budget;
   int64_t u = 0;
@@ -889,8 +893,8 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     vd_plan pl;
     pl.eng = e;
     pl.params = *p;
-    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, pl.chunk);
-    else build_region_chunk(b, u, u_end, e->htab, offsets, pl.chunk);
+    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk);
+    else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk);
     HostChunk& c = pl.chunk;
     pl.L = layout_for(c, b, warps);
     s.host_ms += now_ms() - th;
@@ -950,9 +954,9 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
   if (b->pair_read) {
     PairGroups pg;
     group_pairs(b, pg);
-    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, pl->chunk);
+    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, p->anchored != 0, pl->chunk);
   } else {
-    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, pl->chunk);
+    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, p->anchored != 0, pl->chunk);
   }
   pl->L = layout_for(pl->chunk, b, max_grid_warps(e));
   if ((rc = pl->own.reserve(pl->L.total))) { delete pl; return rc; }

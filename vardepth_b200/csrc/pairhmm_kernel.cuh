@@ -45,9 +45,9 @@ struct LaneRows {
 };
 
 // One DP column of this lane.  s_top is s of the row above at column j-1,
-// u_top is u of the row above at column j.  The row RN values are tapped for
-// the final row sums.
-template <typename T, int R, int RN, bool GEN>
+// u_top is u of the row above at column j.  With TAP the bottom row's mu, nu
+// and omega are returned for the anchored end cell.
+template <typename T, int R, bool GEN, bool TAP>
 __device__ __forceinline__ void column(LaneRows<T, R, GEN>& w, uint32_t hb, T s_top, T u_top,
                                        T k2, T x, T& u_bot, T& tap_mu, T& tap_nu, T& tap_om) {
   T s_above = s_top;
@@ -63,7 +63,7 @@ __device__ __forceinline__ void column(LaneRows<T, R, GEN>& w, uint32_t hb, T s_
     const T om_new = fmaT(x, w.om[r], w.mu[r]);
     const T u_new = fmaT(w.X[r], nu, mu_new);
     const T s_new = fmaT(k2, om_new, fmaT(w.K[r], nu, mu_new));
-    if (r == RN) { tap_mu = mu_new; tap_nu = nu; tap_om = om_new; }
+    if (TAP && r == R - 1) { tap_mu = mu_new; tap_nu = nu; tap_om = om_new; }
     s_above = w.s[r];
     w.mu[r] = mu_new;
     w.om[r] = om_new;
@@ -92,7 +92,19 @@ __device__ __forceinline__ void spill_pair(const QueueView& qv, int32_t read, in
 
 constexpr int kUnroll = 4;
 
-template <typename T, int R, int RN, bool GEN, bool ANCH>
+// Row layout of one read (lane L, register r of strip s holds row
+// i = s*32R + L*R + r - v, 0-based):
+//  * semiglobal (v = 0): rows below the read pass the last row's u down the
+//    column (miss = 0, K = 0, X = 1), and the last row's X is alpha*f_n, so
+//    lane 31's bottom u is the scaled (M + I)[n][j] the result sums;
+//  * anchored: the read ends at lane 31's bottom register of the last strip and
+//    v >= 1 virtual rows sit on top: "zero rows" (miss = K = X = 0) and, just
+//    above row 1, an emulator of row 0 (miss = 1, K = X = 0) that is fed
+//    s(-1) = c at each column 0; its omega recurrence regenerates the anchored
+//    row-0 deletions D[0][j] = g x^(j-1) (anchored.cpp:9).
+constexpr uint32_t kNeverBase = 0x10000u;  // compares unequal to every base byte
+
+template <typename T, int R, bool GEN, bool ANCH>
 __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv, const ItemRef it,
                                           const Tables<T>* __restrict__ tb, const Scalars<T> sc,
                                           const int lane, typename Vec2<T>::type* __restrict__ scratch) {
@@ -106,9 +118,9 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   const uint8_t* __restrict__ rqual = bv.read_quals + roff;
   const int K = w.nhap;
   constexpr int SR = kWarp * R;
-  const int nstrips = (n + SR - 1) / SR;
-  const int last_local = (n - 1) - (nstrips - 1) * SR;
-  const int Ln = last_local / R;  // lane holding row n; RN == last_local % R
+  const int n_rows = n + (ANCH ? 1 : 0);
+  const int nstrips = (n_rows + SR - 1) / SR;
+  const int v = ANCH ? nstrips * SR - n : 0;
 
   auto hap_index = [&](int k) -> int64_t {
     return it.use_sel ? (int64_t)bv.hap_sel[w.hap_begin + k] : w.hap_begin + k;
@@ -131,23 +143,26 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   for (int strip = 0; strip < nstrips; ++strip) {
     const bool last = (strip == nstrips - 1);
     LaneRows<T, R, GEN> rw;
-    const int row0 = strip * SR + lane * R;
+    const int row0 = strip * SR + lane * R - v;
+    int emu = -1;  // register of the anchored row-0 emulator in this lane
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = row0 + r;
-      if (i < n) {
+      if (i >= 0 && i < n) {
         const unsigned q = rqual[i];
         rw.rb[r] = rbase[i];
         rw.miss[r] = tb->miss[q];
         if (GEN) rw.hit[r] = tb->hit[q];
         rw.K[r] = tb->K[q];
-        rw.X[r] = tb->X[q];
+        rw.X[r] = (!ANCH && i == n - 1) ? A : tb->X[q];
       } else {
-        rw.rb[r] = 0u;
-        rw.miss[r] = T(0);
-        if (GEN) rw.hit[r] = T(0);
+        const bool emulator = ANCH && i == -1;
+        if (emulator) emu = r;
+        rw.rb[r] = kNeverBase;
+        rw.miss[r] = emulator ? T(1) : T(0);
+        if (GEN) rw.hit[r] = rw.miss[r];
         rw.K[r] = T(0);
-        rw.X[r] = T(0);
+        rw.X[r] = (!ANCH && i >= n) ? T(1) : T(0);
       }
       rw.mu[r] = T(0);
       rw.om[r] = T(0);
@@ -159,7 +174,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     int S_cur = -1;         // stream position of this lane's current column 0
     const uint8_t* hp = bv.hap_bases;  // hp[p] = haplotype base at stream position p
     T s_top = T(0), u_bot = T(0);
-    T acc32 = T(0), cap = T(0), rmax = T(0), dinj = T(0), bmax = T(0);
+    T acc32 = T(0), cap = T(0), rmax = T(0), bmax = T(0);
     double acc64 = 0.0;
 
     auto finalize = [&](int k) {
@@ -189,16 +204,24 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       acc64 = 0.0;
       cap = T(0);
       rmax = T(0);
+      if (ANCH && strip == 0) {
+        // the emulator row reads s(-1) = c from the row above at column 0
+        if (emu == 0) s_top = c0;
+#pragma unroll
+        for (int r = 1; r < R; ++r)
+          if (emu == r) rw.s[r - 1] = c0;
+      }
     };
 
-    // the final-row tap: semiglobal sums (M + I) over every column, anchored
-    // keeps (M + I + D) of the latest column
+    // the final-row tap (lane 31): semiglobal sums (M + I)[n][j] over every
+    // column -- it arrives as the bottom u -- and anchored keeps (M + I + D) of
+    // the latest column and the running row maximum
     auto accumulate = [&](T tmu, T tnu, T tom) {
       if (ANCH) {
         cap = fmaT(gfin, tom, fmaT(A, tnu, tmu));
         rmax = maxT(rmax, cap);
       } else {
-        acc32 += fmaT(A, tnu, tmu);
+        acc32 += u_bot;
       }
     };
 
@@ -208,7 +231,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       T u_in = __shfl_up_sync(FULL, u_bot, 1);
       T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
       if (p == next_reset) {
-        if (last && kL >= 0 && lane == Ln) finalize(kL);
+        if (last && kL >= 0 && lane == kWarp - 1) finalize(kL);
         ++kL;
         zero_state();
         S_cur = p;
@@ -227,12 +250,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       const uint32_t hb = (active && !col0) ? (uint32_t)hp[p] : 0u;
       T iu, is;
       if (strip == 0) {
-        if (ANCH) {
-          if (col0) { iu = c0; is = c0; dinj = k2 * c0; }
-          else { iu = T(0); is = dinj; dinj *= x; }
-        } else {
-          iu = c0; is = c0;
-        }
+        iu = ANCH ? T(0) : c0;
+        is = iu;
       } else {
         T2 rec = {T(0), T(0)};
         if (lane == 0 && active) rec = scratch[p];
@@ -241,7 +260,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       }
       if (lane == 0) { u_in = iu; s_in = is; }
       T tmu = T(0), tnu = T(0), tom = T(0);
-      column<T, R, RN, GEN>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
+      column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
       s_top = s_in;
       if (last) {
         accumulate(tmu, tnu, tom);
@@ -261,8 +280,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
       T iu, is;
       if (strip == 0) {
-        if (ANCH) { iu = T(0); is = dinj; dinj *= x; }
-        else { iu = c0; is = c0; }
+        iu = ANCH ? T(0) : c0;
+        is = iu;
       } else {
         T2 rec = {T(0), T(0)};
         if (lane == 0) rec = scratch[p];
@@ -271,7 +290,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       }
       if (lane == 0) { u_in = iu; s_in = is; }
       T tmu = T(0), tnu = T(0), tom = T(0);
-      column<T, R, RN, GEN>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
+      column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
       s_top = s_in;
       if (last) {
         accumulate(tmu, tnu, tom);
@@ -351,41 +370,21 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   __syncwarp();
 }
 
-template <typename T, int R, bool ANCH>
-__device__ __forceinline__ void dispatch_rn(int RN, bool gen, const BatchView& bv, const QueueView& qv,
-                                            const ItemRef& it, const Tables<T>* tb, const Scalars<T>& sc,
-                                            int lane, typename Vec2<T>::type* scratch) {
-#define VD_CASE(rn)                                                                        \
-  case rn:                                                                                 \
-    if constexpr ((rn) < R) {                                                              \
-      if (gen) process_item<T, R, (rn), true, ANCH>(bv, qv, it, tb, sc, lane, scratch);    \
-      else process_item<T, R, (rn), false, ANCH>(bv, qv, it, tb, sc, lane, scratch);       \
-    }                                                                                      \
-    break;
-  switch (RN) {
-    VD_CASE(0) VD_CASE(1) VD_CASE(2) VD_CASE(3) VD_CASE(4) VD_CASE(5) VD_CASE(6) VD_CASE(7)
-    default: break;
-  }
-#undef VD_CASE
-}
-
 template <typename T, bool ANCH>
 __device__ __forceinline__ void dispatch(int code, const BatchView& bv, const QueueView& qv,
                                          const ItemRef& it, const Tables<T>* tb, const Scalars<T>& sc,
                                          int lane, typename Vec2<T>::type* scratch) {
-  const int R = code_R(code), RN = code_RN(code);
   const bool gen = code_general(code);
-  switch (R) {
-    case 1: dispatch_rn<T, 1, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 2: dispatch_rn<T, 2, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 3: dispatch_rn<T, 3, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 4: dispatch_rn<T, 4, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 5: dispatch_rn<T, 5, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 6: dispatch_rn<T, 6, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 7: dispatch_rn<T, 7, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
-    case 8: dispatch_rn<T, 8, ANCH>(RN, gen, bv, qv, it, tb, sc, lane, scratch); break;
+#define VD_CASE(r)                                                                   \
+  case r:                                                                            \
+    if (gen) process_item<T, r, true, ANCH>(bv, qv, it, tb, sc, lane, scratch);      \
+    else process_item<T, r, false, ANCH>(bv, qv, it, tb, sc, lane, scratch);         \
+    break;
+  switch (code_R(code)) {
+    VD_CASE(1) VD_CASE(2) VD_CASE(3) VD_CASE(4) VD_CASE(5) VD_CASE(6) VD_CASE(7) VD_CASE(8)
     default: break;
   }
+#undef VD_CASE
 }
 
 // Persistent kernel: every warp pulls work from qv.head until the list is
@@ -435,7 +434,7 @@ pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restri
       it.w.out_begin = e.out;
       it.use_sel = false;
       const int rc = bv.read_code[e.read];
-      code = (tier >= 2) ? make_code(1, 0, code_general(rc), true) : rc;
+      code = (tier >= 2) ? make_code(1, code_general(rc), true) : rc;
       it.w.code = code;
     }
     dispatch<T, ANCH>(code, bv, qv, it, &tab, sc, lane, scratch);
