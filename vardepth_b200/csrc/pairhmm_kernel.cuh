@@ -3,6 +3,7 @@
 #pragma once
 #include <climits>
 #include <cmath>
+#include <type_traits>
 #include "pairhmm_core.cuh"
 
 namespace vd {
@@ -140,8 +141,13 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   int E = 0;          // total power-of-two renormalisation of the strips
   bool fail = false;  // a strip boundary underflowed
 
-  for (int strip = 0; strip < nstrips; ++strip) {
-    const bool last = (strip == nstrips - 1);
+  // One strip of rows.  FIRST and LAST are compile-time tags, so the steady
+  // loop carries no per-step test of the strip position.  Returns false when
+  // the strip's bottom boundary underflowed.
+  auto run_strip = [&](auto first_tag, auto last_tag, const int strip) -> bool {
+    constexpr bool FIRST = decltype(first_tag)::value;
+    constexpr bool last = decltype(last_tag)::value;
+    const bool lane0 = lane == 0;
     LaneRows<T, R, GEN> rw;
     const int row0 = strip * SR + lane * R - v;
     int emu = -1;  // register of the anchored row-0 emulator in this lane
@@ -204,7 +210,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       acc64 = 0.0;
       cap = T(0);
       rmax = T(0);
-      if (ANCH && strip == 0) {
+      if (ANCH && FIRST) {
         // the emulator row reads s(-1) = c from the row above at column 0
         if (emu == 0) s_top = c0;
 #pragma unroll
@@ -249,7 +255,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       const bool col0 = p == S_cur;
       const uint32_t hb = (active && !col0) ? (uint32_t)hp[p] : 0u;
       T iu, is;
-      if (strip == 0) {
+      if (FIRST) {
         iu = ANCH ? T(0) : c0;
         is = iu;
       } else {
@@ -258,7 +264,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         iu = rec.y;
         is = rec.x;
       }
-      if (lane == 0) { u_in = iu; s_in = is; }
+      u_in = lane0 ? iu : u_in;
+      s_in = lane0 ? is : s_in;
       T tmu = T(0), tnu = T(0), tom = T(0);
       column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
       s_top = s_in;
@@ -279,7 +286,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       T u_in = __shfl_up_sync(FULL, u_bot, 1);
       T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
       T iu, is;
-      if (strip == 0) {
+      if (FIRST) {
         iu = ANCH ? T(0) : c0;
         is = iu;
       } else {
@@ -288,7 +295,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         iu = rec.y;
         is = rec.x;
       }
-      if (lane == 0) { u_in = iu; s_in = is; }
+      u_in = lane0 ? iu : u_in;
+      s_in = lane0 ? is : s_in;
       T tmu = T(0), tnu = T(0), tom = T(0);
       column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
       s_top = s_in;
@@ -334,10 +342,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       // so that any exponent shift stays representable
       __syncwarp();
       const T bm = __shfl_sync(FULL, bmax, kWarp - 1);
-      if (!(bm >= sc.strip_floor) || !(bm < T(HUGE_VAL))) {
-        fail = true;
-        break;
-      }
+      if (!(bm >= sc.strip_floor) || !(bm < T(HUGE_VAL))) return false;
       const int ks = sc.target_log2 - ilogb(bm);
       const int k1 = ks / 2;
       const T f1 = pow2T(k1, T(0)), f2 = pow2T(ks - k1, T(0));
@@ -350,6 +355,18 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       __syncwarp();
       E += ks;
     }
+    return true;
+  };
+
+  if (nstrips == 1) {
+    run_strip(std::true_type{}, std::true_type{}, 0);
+  } else if constexpr (R == kMaxR || R == 1) {
+    bool ok = run_strip(std::true_type{}, std::false_type{}, 0);
+    for (int strip = 1; ok && strip < nstrips - 1; ++strip) ok = run_strip(std::false_type{}, std::false_type{}, strip);
+    if (ok) ok = run_strip(std::false_type{}, std::true_type{}, nstrips - 1);
+    fail = !ok;
+  } else {
+    fail = true;  // not reached: reads longer than one strip run with R = 8 (R = 1 in the robust tier)
   }
 
   if (fail) {
