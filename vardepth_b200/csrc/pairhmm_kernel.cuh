@@ -408,8 +408,14 @@ __device__ __forceinline__ void dispatch(int code, const BatchView& bv, const Qu
 // exhausted.  tier 0 reads WorkItems; tiers 1 and 2 read the rescue list the
 // previous tier spilled (one haplotype per entry).  Tier 2 runs R = 1 (strips
 // of 32 rows, renormalised between strips), which no input can underflow.
+// Resident blocks per SM the compiler must fit: the FP32 kernel is issue
+// bound and gains from 20 warps per SM (96 registers); the FP64 tiers keep
+// their registers.
+template <typename T> struct MinBlocks { static constexpr int value = 1; };
+template <> struct MinBlocks<float> { static constexpr int value = 5; };
+
 template <typename T, bool ANCH>
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, MinBlocks<T>::value)
 pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restrict__ gtab,
                const Scalars<T> sc, const int tier) {
   __shared__ Tables<T> tab;
