@@ -47,8 +47,9 @@ struct WorkItem {
   int32_t nhap;       // haplotypes in the list
   int64_t hap_begin;  // first haplotype (contiguous lists) or offset into hap_sel
   int64_t out_begin;  // output slot of the first haplotype, or offset into out_sel
-  int32_t code;       // R | general << 8 | multistrip << 9
-  int32_t tier;       // 0 primary, 1 rescue (FP64), 2 robust (FP64, R = 1)
+  int32_t code;       // R | general << 8 | multistrip << 9 | paired << 10
+  int32_t read2;      // second read of a paired item (same region and R), else -1
+  int64_t out2_begin; // output slot of the second read's first haplotype
 };
 
 // A pair sent to the next precision tier.
@@ -60,9 +61,11 @@ struct RescueEntry {
 
 inline __host__ __device__ int code_R(int c) { return c & 15; }
 inline __host__ __device__ bool code_general(int c) { return (c >> 8) & 1; }
+inline __host__ __device__ bool code_paired(int c) { return (c >> 10) & 1; }
 inline __host__ __device__ int make_code(int R, bool general, bool multistrip) {
   return R | (general ? 256 : 0) | (multistrip ? 512 : 0);
 }
+constexpr int kPairedBit = 1024;
 
 // Per-quality tables (index = raw Phred byte) and scalar constants for one
 // (gap, ext, offsets) setting, in the arithmetic type of the kernel.

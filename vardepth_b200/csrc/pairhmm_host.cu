@@ -152,6 +152,7 @@ struct vd_engine {
   cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
   std::mutex mu;
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
+  int grid_pair = 0;                  // blocks of the two-read kernel
   // table cache
   TableKey tkey{};
   bool tvalid = false;
@@ -269,6 +270,7 @@ struct HostChunk {
   int max_hap = 0;
   bool any_long = false;           // a read longer than 32 (the robust tier strip-mines it)
   bool any_strip = false;          // a read longer than one 256-row strip (every tier strip-mines it)
+  int64_t n_paired = 0;            // leading items that carry two reads (own kernel)
 };
 
 // The robust tier runs on a small grid: it only sees pairs the FP64 wavefront
@@ -373,8 +375,13 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
 // Work items of a region chunk: one item per read with the region's non-empty
 // haplotypes as contiguous runs; reads longer than a strip get one item per
 // haplotype (their strip boundary scratch holds one haplotype).
+// Work items of a region chunk: one item per read with the region's non-empty
+// haplotypes as contiguous runs; reads longer than a strip get one item per
+// haplotype (their strip boundary scratch holds one haplotype).  With
+// pair_reads, two reads of a region with the same kernel variant (single strip,
+// one-sided emission) share an item and run in the packed two-read path.
 void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSet* ts, bool offsets,
-                        bool anchored, HostChunk& c) {
+                        bool anchored, bool pair_reads, HostChunk& c) {
   c.ra = b->region_read_off[g0];
   c.rb = b->region_read_off[g1];
   c.ha = b->region_hap_off[g0];
@@ -390,10 +397,12 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
     const int64_t r_lo = b->region_read_off[g], r_hi = b->region_read_off[g + 1];
     const int64_t h_lo = b->region_hap_off[g], h_hi = b->region_hap_off[g + 1];
     const int64_t nh = h_hi - h_lo;
-    for (int64_t r = r_lo; r < r_hi; ++r, out += nh) {
+    const int64_t region_out = out;
+    // emit the haplotype runs of read r (and r2 >= 0 riding along)
+    auto emit = [&](int64_t r, int64_t r2) {
       const int32_t code = c.read_code[r - c.ra];
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
-      if (n <= 0) continue;
+      const int n2 = r2 >= 0 ? (int)(c.read_off[r2 - c.ra + 1] - c.read_off[r2 - c.ra]) : 0;
       const int R = code_R(code);
       const int n_rows = n + (anchored ? 1 : 0);
       const int64_t rows = (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R));
@@ -408,25 +417,48 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
           if (m <= 0) break;
           if (run_end > h && (multistrip || stream + m + 1 > kMaxStream)) break;
           stream += m + 1;
-          c.cells += (int64_t)n * m;
-          ++c.pairs_scored;
+          c.cells += (int64_t)(n + n2) * m;
+          c.pairs_scored += r2 >= 0 ? 2 : 1;
           ++run_end;
         }
         WorkItem w;
         w.read = (int32_t)(r - c.ra);
         w.nhap = (int32_t)(run_end - h);
         w.hap_begin = h - c.ha;
-        w.out_begin = out + (h - h_lo);
-        w.code = code;
-        w.tier = 0;
+        w.out_begin = region_out + (r - r_lo) * nh + (h - h_lo);
+        w.code = r2 >= 0 ? (code | kPairedBit) : code;
+        w.read2 = r2 >= 0 ? (int32_t)(r2 - c.ra) : -1;
+        w.out2_begin = r2 >= 0 ? region_out + (r2 - r_lo) * nh + (h - h_lo) : 0;
         c.items.push_back(w);
-        cost.push_back(rows * (stream + kWarp));
+        cost.push_back(rows * (stream + kWarp) * (r2 >= 0 ? 2 : 1));
         h = run_end;
       }
+    };
+    int64_t waiting[kMaxR + 1];
+    for (int k = 0; k <= kMaxR; ++k) waiting[k] = -1;
+    for (int64_t r = r_lo; r < r_hi; ++r) {
+      const int32_t code = c.read_code[r - c.ra];
+      const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
+      if (n <= 0) continue;
+      const bool eligible = pair_reads && !anchored && !code_general(code) && (code & 512) == 0;
+      if (!eligible) { emit(r, -1); continue; }
+      const int R = code_R(code);
+      if (waiting[R] >= 0) {
+        emit(waiting[R], r);
+        waiting[R] = -1;
+      } else {
+        waiting[R] = r;
+      }
     }
+    for (int k = 0; k <= kMaxR; ++k)
+      if (waiting[k] >= 0) emit(waiting[k], -1);
+    out += (r_hi - r_lo) * nh;
   }
   c.n_out = out;
   order_items(c.items, cost);
+  auto mid = std::stable_partition(c.items.begin(), c.items.end(),
+                                   [](const WorkItem& w) { return code_paired(w.code); });
+  c.n_paired = (int64_t)(mid - c.items.begin());
 }
 
 // Pair form: pairs grouped by read (counting sort), each read's haplotypes as
@@ -472,7 +504,8 @@ void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64
       w.hap_begin = list_begin;
       w.out_begin = list_begin;
       w.code = code;
-      w.tier = 0;
+      w.read2 = -1;
+        w.out2_begin = 0;
       c.items.push_back(w);
       cost.push_back(rows * (stream + kWarp));
       list_begin = (int64_t)c.hap_sel.size();
@@ -554,6 +587,7 @@ struct vd_plan {
   double offsets[4] = {0, 0, 0, 0};
   bool has_offsets = false;
   cudaGraphExec_t graph = nullptr;
+  int graph_launches = 0;  // kernels in the captured graph
   int64_t last_rescued1 = 0, last_rescued2 = 0;
 };
 
@@ -642,10 +676,25 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   q.spill_cap = cap;
   int n = 0;
   if (!pl->chunk.items.empty()) {
-    cudaError_t err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], e->stream)
-                          : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], e->stream);
-    if (err != cudaSuccess) return cuda_fail(err, "primary tier launch");
-    ++n;
+    cudaError_t err = cudaSuccess;
+    const int64_t np = pl->chunk.n_paired;
+    if (np > 0) {
+      // two-read items first, on their own kernel (FP32 semiglobal only)
+      QueueView qp = q;
+      qp.n_items = np;
+      qp.head = cnt + 6;
+      err = launch_pair_f32(bv, qp, &dt->f32, ht->s32, e->grid_pair, e->stream);
+      if (err != cudaSuccess) return cuda_fail(err, "two-read tier launch");
+      ++n;
+    }
+    q.items = (const WorkItem*)(d + L.o_items) + np;
+    q.n_items = (long long)(pl->chunk.items.size() - np);
+    if (q.n_items > 0) {
+      err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], e->stream)
+                : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], e->stream);
+      if (err != cudaSuccess) return cuda_fail(err, "primary tier launch");
+      ++n;
+    }
     VD_CUDA(cudaEventRecordWithFlags(e->ev_mid, e->stream, evflags));
     BatchView rv = bv;
     rv.hap_sel = nullptr;
@@ -715,6 +764,10 @@ int init_engine_grids(vd_engine* e) {
       if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
       e->grid[f][a] = std::max(1, bps) * e->sm_count;
     }
+  int bps = 0;
+  cudaError_t err = occupancy_pair_f32(&bps);
+  if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+  e->grid_pair = std::max(1, bps) * e->sm_count;
   return VD_OK;
 }
 
@@ -894,7 +947,7 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     pl.eng = e;
     pl.params = *p;
     if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk);
-    else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk);
+    else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED, pl.chunk);
     HostChunk& c = pl.chunk;
     pl.L = layout_for(c, b, warps);
     s.host_ms += now_ms() - th;
@@ -956,7 +1009,7 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
     group_pairs(b, pg);
     build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, p->anchored != 0, pl->chunk);
   } else {
-    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, p->anchored != 0, pl->chunk);
+    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED, pl->chunk);
   }
   pl->L = layout_for(pl->chunk, b, max_grid_warps(e));
   if ((rc = pl->own.reserve(pl->L.total))) { delete pl; return rc; }
@@ -987,11 +1040,12 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
     cudaError_t err = cudaStreamEndCapture(e->stream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     if (err != cudaSuccess) return cuda_fail(err, "graph capture");
+    pl->graph_launches = launches;
     err = cudaGraphInstantiate(&pl->graph, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) { pl->graph = nullptr; return cuda_fail(err, "graph instantiate"); }
   } else {
-    launches = pl->chunk.items.empty() ? 0 : (pl->params.precision == VD_PRECISION_FLOAT64 ? 2 : 3);
+    launches = pl->graph_launches;
   }
   VD_CUDA(cudaGraphLaunch(pl->graph, e->stream));
   int64_t r1 = 0, r2 = 0;

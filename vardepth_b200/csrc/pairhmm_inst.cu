@@ -35,4 +35,17 @@ cudaError_t VD_NAME(occupancy, VD_TNAME, VD_MNAME)(int* blocks_per_sm) {
                                                        kWarpsPerBlock * kWarp, 0);
 }
 
+#if !VD_FP64 && !VD_ANCH
+cudaError_t launch_pair_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
+                            const Scalars<float>& sc, int grid, cudaStream_t stream) {
+  pairhmm_pair_kernel<0><<<grid, kWarpsPerBlock * kWarp, 0, stream>>>(bv, qv, tab, sc);
+  return cudaGetLastError();
+}
+
+cudaError_t occupancy_pair_f32(int* blocks_per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<0>,
+                                                       kWarpsPerBlock * kWarp, 0);
+}
+#endif
+
 }  // namespace vd

@@ -387,6 +387,210 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   __syncwarp();
 }
 
+// ---- two reads per warp (FP32, semiglobal, one strip) -------------------------
+// Two reads of one region with the same rows per lane advance together through
+// the region's haplotype stream.  Their rows are packed as float2, so every FMA
+// serves both reads (fma.rn.f32x2): per two cells 2 compares, 2 predicated
+// multiplies and 4 packed FMAs instead of 12 scalar instructions, and the
+// haplotype base load, the ramp and the per-step bookkeeping are shared.
+template <int R>
+struct PairRows {
+  uint32_t ra[R], rb[R];       // read bases of the two reads
+  float2 miss[R], K[R], X[R];  // per-row factors (x: first read, y: second)
+  float2 mu[R], om[R], s[R];   // state of the previous column
+};
+
+template <int R>
+__device__ __forceinline__ void column2(PairRows<R>& w, uint32_t hb, float2 s_top, float2 u_top, float2 k2,
+                                        float2 x, float2& u_bot) {
+  float2 s_above = s_top;
+  float2 nu = u_top;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    float2 mu_new = s_above;
+    mul_if_ne(mu_new.x, w.ra[r], hb, w.miss[r].x);
+    mul_if_ne(mu_new.y, w.rb[r], hb, w.miss[r].y);
+    const float2 om_new = __ffma2_rn(x, w.om[r], w.mu[r]);
+    const float2 u_new = __ffma2_rn(w.X[r], nu, mu_new);
+    const float2 s_new = __ffma2_rn(k2, om_new, __ffma2_rn(w.K[r], nu, mu_new));
+    s_above = w.s[r];
+    w.mu[r] = mu_new;
+    w.om[r] = om_new;
+    w.s[r] = s_new;
+    nu = u_new;
+  }
+  u_bot = nu;
+}
+
+__device__ __forceinline__ float2 shfl_up2(float2 v) {
+  return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
+}
+
+template <int R>
+__device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv, const ItemRef it,
+                                          const Tables<float>* __restrict__ tb, const Scalars<float> sc,
+                                          const int lane) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr double kLn2 = 0.6931471805599453094;
+  const WorkItem& w = it.w;
+  const int64_t offA = bv.read_off[w.read], offB = bv.read_off[w.read2];
+  const int nA = (int)(bv.read_off[w.read + 1] - offA);
+  const int nB = (int)(bv.read_off[w.read2 + 1] - offB);
+  const uint8_t* __restrict__ bA = bv.read_bases + offA;
+  const uint8_t* __restrict__ qA = bv.read_quals + offA;
+  const uint8_t* __restrict__ bB = bv.read_bases + offB;
+  const uint8_t* __restrict__ qB = bv.read_quals + offB;
+  const int K = w.nhap;
+
+  double lnA = 0.0, lnB = 0.0;
+  for (int i = lane; i < nA; i += kWarp) lnA += tb->lnN[qA[i]];
+  for (int i = lane; i < nB; i += kWarp) lnB += tb->lnN[qB[i]];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    lnA += __shfl_xor_sync(FULL, lnA, o);
+    lnB += __shfl_xor_sync(FULL, lnB, o);
+  }
+  const float AA = tb->A[qA[nA - 1]], AB = tb->A[qB[nB - 1]];
+  const float2 k2 = make_float2(sc.k2, sc.k2), x = make_float2(sc.x, sc.x);
+  const float2 c2 = make_float2(sc.c, sc.c);
+  const bool lane0 = lane == 0;
+
+  // rows as process_item lays out a semiglobal read: the last row's X is
+  // alpha*f_n and padding rows pass u down the column
+  PairRows<R> rw;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = lane * R + r;
+    if (i < nA) {
+      const unsigned q = qA[i];
+      rw.ra[r] = bA[i];
+      rw.miss[r].x = tb->miss[q];
+      rw.K[r].x = tb->K[q];
+      rw.X[r].x = (i == nA - 1) ? AA : tb->X[q];
+    } else {
+      rw.ra[r] = kNeverBase;
+      rw.miss[r].x = 0.f;
+      rw.K[r].x = 0.f;
+      rw.X[r].x = 1.f;
+    }
+    if (i < nB) {
+      const unsigned q = qB[i];
+      rw.rb[r] = bB[i];
+      rw.miss[r].y = tb->miss[q];
+      rw.K[r].y = tb->K[q];
+      rw.X[r].y = (i == nB - 1) ? AB : tb->X[q];
+    } else {
+      rw.rb[r] = kNeverBase;
+      rw.miss[r].y = 0.f;
+      rw.K[r].y = 0.f;
+      rw.X[r].y = 1.f;
+    }
+    rw.mu[r] = make_float2(0.f, 0.f);
+    rw.om[r] = make_float2(0.f, 0.f);
+    rw.s[r] = make_float2(0.f, 0.f);
+  }
+
+  int kL = -1, next_reset = 0, S_cur = -1;
+  const uint8_t* hp = bv.hap_bases;
+  float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
+  double accA = 0.0, accB = 0.0;
+
+  auto finalize = [&](int k) {
+    const int64_t h = w.hap_begin + k;
+    const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
+    const double lnC0 = sc.ln_c + log((double)(m + 1));
+    const double za = accA + (double)acc32.x, zb = accB + (double)acc32.y;
+    const int64_t oa = w.out_begin + k, ob = w.out2_begin + k;
+    if (za >= (double)sc.final_floor && za < HUGE_VAL) {
+      bv.out[oa] = log(za) - lnC0 + lnA;
+    } else {
+      bv.out[oa] = __longlong_as_double(0x7ff8000000000000LL);
+      spill_pair<float>(qv, w.read, h, oa);
+    }
+    if (zb >= (double)sc.final_floor && zb < HUGE_VAL) {
+      bv.out[ob] = log(zb) - lnC0 + lnB;
+    } else {
+      bv.out[ob] = __longlong_as_double(0x7ff8000000000000LL);
+      spill_pair<float>(qv, w.read2, h, ob);
+    }
+  };
+
+  auto flush = [&]() {
+    accA += (double)acc32.x;
+    accB += (double)acc32.y;
+    acc32 = make_float2(0.f, 0.f);
+  };
+
+  auto gstep = [&](int t) {
+    const int p = t - lane;
+    float2 u_in = shfl_up2(u_bot);
+    float2 s_in = shfl_up2(rw.s[R - 1]);
+    if (p == next_reset) {
+      if (kL >= 0 && lane == kWarp - 1) finalize(kL);
+      ++kL;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        rw.mu[r] = make_float2(0.f, 0.f);
+        rw.om[r] = make_float2(0.f, 0.f);
+        rw.s[r] = make_float2(0.f, 0.f);
+      }
+      s_top = make_float2(0.f, 0.f);
+      acc32 = make_float2(0.f, 0.f);
+      accA = accB = 0.0;
+      S_cur = p;
+      if (kL < K) {
+        const int64_t h = w.hap_begin + kL;
+        const int64_t ho = bv.hap_off[h];
+        hp = bv.hap_bases + ho - 1 - p;
+        next_reset = p + (int)(bv.hap_off[h + 1] - ho) + 1;
+      } else {
+        next_reset = INT_MAX;
+      }
+    }
+    const bool active = kL >= 0 && kL < K;
+    const uint32_t hb = (active && p != S_cur) ? (uint32_t)hp[p] : 0u;
+    u_in = lane0 ? c2 : u_in;
+    s_in = lane0 ? c2 : s_in;
+    column2<R>(rw, hb, s_top, u_in, k2, x, u_bot);
+    s_top = s_in;
+    acc32 = __fadd2_rn(acc32, u_bot);
+    flush();
+  };
+
+  auto sstep = [&](uint32_t hb) {
+    float2 u_in = shfl_up2(u_bot);
+    float2 s_in = shfl_up2(rw.s[R - 1]);
+    u_in = lane0 ? c2 : u_in;
+    s_in = lane0 ? c2 : s_in;
+    column2<R>(rw, hb, s_top, u_in, k2, x, u_bot);
+    s_top = s_in;
+    acc32 = __fadd2_rn(acc32, u_bot);
+  };
+
+  int t = 0, S = 0;
+  for (int k = 0; k <= K; ++k) {
+    int mk = 0;
+    if (k < K) mk = (int)(bv.hap_off[w.hap_begin + k + 1] - bv.hap_off[w.hap_begin + k]);
+    const int Snext = S + mk + 1;
+    const int gen_end = (k < K) ? min(S + kWarp, Snext) : S + kWarp;
+    for (; t < gen_end; ++t) gstep(t);
+    if (k < K) {
+      for (; t + kUnroll <= Snext; t += kUnroll) {
+        const uint8_t* q = hp + (t - lane);
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) sstep((uint32_t)q[u]);
+        flush();
+      }
+      for (; t < Snext; ++t) {
+        sstep((uint32_t)hp[t - lane]);
+        flush();
+      }
+    }
+    S = Snext;
+  }
+  __syncwarp();
+}
+
 template <typename T, bool ANCH>
 __device__ __forceinline__ void dispatch(int code, const BatchView& bv, const QueueView& qv,
                                          const ItemRef& it, const Tables<T>* tb, const Scalars<T>& sc,
@@ -455,12 +659,53 @@ pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restri
       it.w.nhap = 1;
       it.w.hap_begin = e.hap;
       it.w.out_begin = e.out;
+      it.w.read2 = -1;
+      it.w.out2_begin = 0;
       it.use_sel = false;
       const int rc = bv.read_code[e.read];
       code = (tier >= 2) ? make_code(1, code_general(rc), true) : rc;
       it.w.code = code;
     }
     dispatch<T, ANCH>(code, bv, qv, it, &tab, sc, lane, scratch);
+  }
+}
+
+// Persistent kernel of the two-read items (FP32, semiglobal).  Its packed
+// rows need about 14 registers each, so it runs 3 blocks per SM on its own
+// work list, ahead of the single-read items of the same tier.
+template <int kUnused = 0>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, 3)
+pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
+                    const Scalars<float> sc) {
+  __shared__ Tables<float> tab;
+  {
+    const int words = (int)(sizeof(Tables<float>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(gtab);
+    int* dst = reinterpret_cast<int*>(&tab);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & (kWarp - 1);
+  for (;;) {
+    unsigned long long i = 0;
+    if (lane == 0) i = atomicAdd(qv.head, 1ull);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if ((long long)i >= qv.n_items) break;
+    ItemRef it;
+    it.w = qv.items[i];
+    it.use_sel = false;
+    it.tier = 0;
+    switch (code_R(it.w.code)) {
+      case 1: process_pair<1>(bv, qv, it, &tab, sc, lane); break;
+      case 2: process_pair<2>(bv, qv, it, &tab, sc, lane); break;
+      case 3: process_pair<3>(bv, qv, it, &tab, sc, lane); break;
+      case 4: process_pair<4>(bv, qv, it, &tab, sc, lane); break;
+      case 5: process_pair<5>(bv, qv, it, &tab, sc, lane); break;
+      case 6: process_pair<6>(bv, qv, it, &tab, sc, lane); break;
+      case 7: process_pair<7>(bv, qv, it, &tab, sc, lane); break;
+      case 8: process_pair<8>(bv, qv, it, &tab, sc, lane); break;
+      default: break;
+    }
   }
 }
 
