@@ -98,9 +98,12 @@ void build_tables(double g, double x, const double* offsets, TableSet* ts) {
     ts->f32.general[q] = gen;     ts->f64.general[q] = gen;
   }
   ts->s32.k2 = (float)k2; ts->s32.x = (float)x; ts->s32.gfin = (float)g;
-  ts->s32.c = std::ldexp(1.0f, 100); ts->s32.ln_c = 100.0 * std::log(2.0);
-  ts->s32.strip_floor = std::ldexp(1.0f, -40); ts->s32.final_floor = std::ldexp(1.0f, -64);
-  ts->s32.target_log2 = 100;
+  // FP32 range: cells stay below ~1.33 c (a row grows by at most 1 + K + k2/(1-x)
+  // ~ 1.0011 over its predecessor), so c = 2^120 leaves 2^7 of headroom; a final
+  // sum >= 2^-80 keeps the dominant cells normal (>= 2^-93 after m+1 <= 2^13 terms)
+  ts->s32.c = std::ldexp(1.0f, 120); ts->s32.ln_c = 120.0 * std::log(2.0);
+  ts->s32.strip_floor = std::ldexp(1.0f, -40); ts->s32.final_floor = std::ldexp(1.0f, -80);
+  ts->s32.target_log2 = 120;
   ts->s64.k2 = k2; ts->s64.x = x; ts->s64.gfin = g;
   ts->s64.c = std::ldexp(1.0, 600); ts->s64.ln_c = 600.0 * std::log(2.0);
   ts->s64.strip_floor = std::ldexp(1.0, -800); ts->s64.final_floor = std::ldexp(1.0, -900);
