@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
@@ -57,6 +58,20 @@ double now_ms() {
 }
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Runs fn(begin, end) over [0, n) in contiguous slices on up to 32 host threads
+// (the calling thread takes the first slice); ranges below 2 grains run inline.
+template <typename F>
+void parallel_for(int64_t n, int64_t grain, F&& fn) {
+  const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+  const int64_t T = std::min<int64_t>(std::min<int64_t>(hw, 32), std::max<int64_t>(1, n / std::max<int64_t>(1, grain)));
+  if (T <= 1) { fn((int64_t)0, n); return; }
+  std::vector<std::thread> th;
+  th.reserve((size_t)T - 1);
+  for (int64_t t = 1; t < T; ++t) th.emplace_back([&fn, n, t, T] { fn(n * t / T, n * (t + 1) / T); });
+  fn((int64_t)0, n / T);
+  for (auto& x : th) x.join();
+}
 
 // ---- model tables -----------------------------------------------------------
 
@@ -166,6 +181,19 @@ struct vd_engine {
   std::vector<double> out_stage;
   // live plans: destroying the engine first releases their device resources
   std::unordered_set<vd_plan*> plans;
+  // vd_forward pipeline: two slots, each with its own stream, arena and events,
+  // so one chunk's host work-list build and upload overlap the other's kernels
+  struct Slot {
+    DevBuf arena;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    unsigned long long* hcnt = nullptr;  // pinned copy of the tier counters
+    std::vector<double> stage;           // pair-form outputs before the scatter
+    vd_plan* pl = nullptr;
+    bool busy = false;
+    int launches = 0;
+  };
+  Slot slots[2];
 };
 
 namespace {
@@ -293,28 +321,33 @@ void order_items(std::vector<WorkItem>& items, const std::vector<int64_t>& cost)
   const int nb = 256;
   std::vector<int> bucket(n);
   for (size_t i = 0; i < n; ++i) {
-    const double c = (double)std::max<int64_t>(1, cost[i]);
-    int k = (int)(std::log2(c) * 4.0);
+    // quarter-octave bucket: floor(log2 c) and the next two bits
+    const uint64_t c = (uint64_t)std::max<int64_t>(4, cost[i]);
+    const int lz = 63 - __builtin_clzll(c);
+    int k = lz * 4 + (int)((c >> (lz - 2)) & 3);
     k = std::max(0, std::min(nb - 1, k));
     bucket[i] = nb - 1 - k;
   }
-  // groups ordered by decreasing mean cost
-  std::unordered_map<int32_t, std::pair<double, int64_t>> stat;
+  // groups ordered by decreasing mean cost (codes are small integers)
+  constexpr int kCodes = 4096;
+  std::vector<double> sum(kCodes, 0.0);
+  std::vector<int64_t> cnt(kCodes, 0);
   for (size_t i = 0; i < n; ++i) {
-    auto& st = stat[items[i].code];
-    st.first += (double)cost[i];
-    st.second += 1;
+    const int cd = items[i].code & (kCodes - 1);
+    sum[cd] += (double)cost[i];
+    cnt[cd] += 1;
   }
   std::vector<std::pair<double, int32_t>> groups;
-  for (auto& kv : stat) groups.push_back({kv.second.first / (double)kv.second.second, kv.first});
+  for (int cd = 0; cd < kCodes; ++cd)
+    if (cnt[cd]) groups.push_back({sum[cd] / (double)cnt[cd], cd});
   std::sort(groups.begin(), groups.end(), [](auto& a, auto& b) { return a.first > b.first || (a.first == b.first && a.second < b.second); });
-  std::unordered_map<int32_t, int> rank;
+  std::vector<int> rank(kCodes, 0);
   for (size_t g = 0; g < groups.size(); ++g) rank[groups[g].second] = (int)g;
   const int ng = (int)groups.size();
   std::vector<int64_t> count((size_t)ng * nb + 1, 0);
   std::vector<int64_t> key(n);
   for (size_t i = 0; i < n; ++i) {
-    key[i] = (int64_t)rank[items[i].code] * nb + bucket[i];
+    key[i] = (int64_t)rank[items[i].code & (kCodes - 1)] * nb + bucket[i];
     ++count[key[i] + 1];
   }
   for (size_t k = 0; k + 1 < count.size(); ++k) count[k + 1] += count[k];
@@ -333,12 +366,12 @@ ReadInfo read_info(const vd_batch* b, int64_t r, bool anchored) {
   const int n = (int)(b->read_off[r + 1] - o);
   ReadInfo ri{n, 0};
   if (n <= 0) return ri;
-  bool gen = false;
+  // P0 > P1 only for Phred 0 and 1 (e > 0.75); offsets can move a bin there.
+  // A branch-free minimum vectorises; an early exit would not.
   const unsigned char* q = b->read_quals + o;
-  for (int i = 0; i < n; ++i) {
-    // P0 > P1 only for Phred 0 and 1 (e > 0.75); offsets can move a bin there
-    if (q[i] < 2) { gen = true; break; }
-  }
+  unsigned char qmin = 255;
+  for (int i = 0; i < n; ++i) qmin = q[i] < qmin ? q[i] : qmin;
+  const bool gen = qmin < 2;
   // anchored reads carry one extra row on top: the emulator of row 0
   const int rows = n + (anchored ? 1 : 0);
   ri.code = make_code(rows_per_lane(rows), gen, rows > kStripRows);
@@ -358,15 +391,22 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
   c.read_off.resize(c.rb - c.ra + 1);
   c.read_code.resize(c.rb - c.ra);
   const int64_t r0 = b->read_off[c.ra];
-  for (int64_t r = c.ra; r <= c.rb; ++r) c.read_off[r - c.ra] = b->read_off[r] - r0;
+  parallel_for(c.rb - c.ra, 4096, [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k) {
+      const int64_t r = c.ra + k;
+      c.read_off[k] = b->read_off[r] - r0;
+      ReadInfo ri = read_info(b, r, anchored);
+      if (offsets && ri.n > 0 && !code_general(ri.code) && read_general(b, r, ts))
+        ri.code |= 256;
+      c.read_code[k] = ri.code;
+    }
+  });
+  c.read_off[c.rb - c.ra] = b->read_off[c.rb] - r0;
   for (int64_t r = c.ra; r < c.rb; ++r) {
-    ReadInfo ri = read_info(b, r, anchored);
-    if (offsets && ri.n > 0 && !code_general(ri.code) && read_general(b, r, ts))
-      ri.code |= 256;
-    c.read_code[r - c.ra] = ri.code;
-    const int rows = ri.n + (anchored ? 1 : 0);
-    if (ri.n > 0 && rows > kWarp) c.any_long = true;
-    if (ri.n > 0 && rows > kStripRows) c.any_strip = true;
+    const int n = (int)(b->read_off[r + 1] - b->read_off[r]);
+    const int rows = n + (anchored ? 1 : 0);
+    if (n > 0 && rows > kWarp) c.any_long = true;
+    if (n > 0 && rows > kStripRows) c.any_strip = true;
   }
   c.hap_off.resize(c.hb - c.ha + 1);
   const int64_t h0 = b->hap_off[c.ha];
@@ -375,9 +415,6 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
   for (int64_t h = c.ha; h < c.hb; ++h) c.max_hap = std::max<int>(c.max_hap, (int)(b->hap_off[h + 1] - b->hap_off[h]));
 }
 
-// Work items of a region chunk: one item per read with the region's non-empty
-// haplotypes as contiguous runs; reads longer than a strip get one item per
-// haplotype (their strip boundary scratch holds one haplotype).
 // Work items of a region chunk: one item per read with the region's non-empty
 // haplotypes as contiguous runs; reads longer than a strip get one item per
 // haplotype (their strip boundary scratch holds one haplotype).  With
@@ -393,14 +430,32 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   for (int64_t g = 0; g < g0; ++g)
     c.out_begin += (b->region_read_off[g + 1] - b->region_read_off[g]) * (b->region_hap_off[g + 1] - b->region_hap_off[g]);
   finish_chunk_common(c, b, ts, offsets, anchored);
-  std::vector<int64_t> cost;
-  int64_t out = 0;
   const int kMaxStream = 1 << 30;
-  for (int64_t g = g0; g < g1; ++g) {
+  // output offset of every region inside the chunk
+  const int64_t ng = g1 - g0;
+  std::vector<int64_t> region_out_of(ng + 1, 0);
+  for (int64_t k = 0; k < ng; ++k)
+    region_out_of[k + 1] = region_out_of[k] + (b->region_read_off[g0 + k + 1] - b->region_read_off[g0 + k]) *
+                                                  (b->region_hap_off[g0 + k + 1] - b->region_hap_off[g0 + k]);
+  // regions are cut into a fixed number of slices (so the result does not
+  // depend on the thread count) and the slices are built in parallel
+  struct Slice {
+    std::vector<WorkItem> items;
+    std::vector<int64_t> cost;
+    int64_t cells = 0, pairs = 0;
+  };
+  const int64_t nslices = std::max<int64_t>(1, std::min<int64_t>(256, ng / 16));
+  std::vector<Slice> slices((size_t)nslices);
+  parallel_for(nslices, 1, [&](int64_t s_lo, int64_t s_hi) {
+   for (int64_t si = s_lo; si < s_hi; ++si) {
+    Slice& sl = slices[(size_t)si];
+    std::vector<WorkItem>& items = sl.items;
+    std::vector<int64_t>& cost = sl.cost;
+    for (int64_t g = g0 + ng * si / nslices; g < g0 + ng * (si + 1) / nslices; ++g) {
     const int64_t r_lo = b->region_read_off[g], r_hi = b->region_read_off[g + 1];
     const int64_t h_lo = b->region_hap_off[g], h_hi = b->region_hap_off[g + 1];
     const int64_t nh = h_hi - h_lo;
-    const int64_t region_out = out;
+    const int64_t region_out = region_out_of[g - g0];
     // emit the haplotype runs of read r (and r2 >= 0 riding along)
     auto emit = [&](int64_t r, int64_t r2) {
       const int32_t code = c.read_code[r - c.ra];
@@ -420,8 +475,8 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
           if (m <= 0) break;
           if (run_end > h && (multistrip || stream + m + 1 > kMaxStream)) break;
           stream += m + 1;
-          c.cells += (int64_t)(n + n2) * m;
-          c.pairs_scored += r2 >= 0 ? 2 : 1;
+          sl.cells += (int64_t)(n + n2) * m;
+          sl.pairs += r2 >= 0 ? 2 : 1;
           ++run_end;
         }
         WorkItem w;
@@ -432,7 +487,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
         w.code = r2 >= 0 ? (code | kPairedBit) : code;
         w.read2 = r2 >= 0 ? (int32_t)(r2 - c.ra) : -1;
         w.out2_begin = r2 >= 0 ? region_out + (r2 - r_lo) * nh + (h - h_lo) : 0;
-        c.items.push_back(w);
+        items.push_back(w);
         cost.push_back(rows * (stream + kWarp) * (r2 >= 0 ? 2 : 1));
         h = run_end;
       }
@@ -455,8 +510,21 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
     }
     for (int k = 0; k <= kMaxR; ++k)
       if (waiting[k] >= 0) emit(waiting[k], -1);
-    out += (r_hi - r_lo) * nh;
+    }
+   }
+  });
+  std::vector<int64_t> cost;
+  size_t total = 0;
+  for (auto& sl : slices) total += sl.items.size();
+  c.items.reserve(total);
+  cost.reserve(total);
+  for (auto& sl : slices) {
+    c.items.insert(c.items.end(), sl.items.begin(), sl.items.end());
+    cost.insert(cost.end(), sl.cost.begin(), sl.cost.end());
+    c.cells += sl.cells;
+    c.pairs_scored += sl.pairs;
   }
+  const int64_t out = region_out_of[ng];
   c.n_out = out;
   order_items(c.items, cost);
   auto mid = std::stable_partition(c.items.begin(), c.items.end(),
@@ -591,6 +659,10 @@ struct vd_plan {
   bool has_offsets = false;
   cudaGraphExec_t graph = nullptr;
   int graph_launches = 0;  // kernels in the captured graph
+  // stream and tier events the plan's work is enqueued on (the engine's own,
+  // or a pipeline slot's in vd_forward)
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
   int64_t last_rescued1 = 0, last_rescued2 = 0;
 };
 
@@ -620,7 +692,7 @@ int upload_chunk(vd_plan* pl, const vd_batch* b, int64_t* h2d) {
   int64_t bytes = 0;
   auto put = [&](size_t off, const void* src, size_t n) -> int {
     if (n == 0) return VD_OK;
-    VD_CUDA(cudaMemcpyAsync(d + off, src, n, cudaMemcpyHostToDevice, e->stream));
+    VD_CUDA(cudaMemcpyAsync(d + off, src, n, cudaMemcpyHostToDevice, pl->stream));
     bytes += (int64_t)n;
     return VD_OK;
   };
@@ -635,7 +707,7 @@ int upload_chunk(vd_plan* pl, const vd_batch* b, int64_t* h2d) {
   if ((rc = put(pl->L.o_osel, c.out_sel.data(), c.out_sel.size() * sizeof(int64_t)))) return rc;
   if ((rc = put(pl->L.o_items, c.items.data(), c.items.size() * sizeof(WorkItem)))) return rc;
   if (c.n_out > 0) {
-    fill_kernel<<<(int)std::min<int64_t>(4096, (c.n_out + 255) / 256), 256, 0, e->stream>>>(
+    fill_kernel<<<(int)std::min<int64_t>(4096, (c.n_out + 255) / 256), 256, 0, pl->stream>>>(
         (double*)(d + pl->L.o_out), c.n_out, -HUGE_VAL);
     VD_CUDA(cudaGetLastError());
   }
@@ -657,8 +729,8 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   cudaGetLastError();  // launch checks below must see only their own errors
   // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag
-  VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), e->stream));
-  VD_CUDA(cudaEventRecordWithFlags(e->ev_begin, e->stream, evflags));
+  VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), pl->stream));
+  VD_CUDA(cudaEventRecordWithFlags(pl->ev_begin, pl->stream, evflags));
   const BatchView bv = batch_view(pl);
   // device tables by address; the scalars by value from the host copy
   TableSet* dt = (TableSet*)e->dtab.p;
@@ -686,19 +758,19 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       QueueView qp = q;
       qp.n_items = np;
       qp.head = cnt + 6;
-      err = launch_pair_f32(bv, qp, &dt->f32, ht->s32, e->grid_pair, e->stream);
+      err = launch_pair_f32(bv, qp, &dt->f32, ht->s32, e->grid_pair, pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "two-read tier launch");
       ++n;
     }
     q.items = (const WorkItem*)(d + L.o_items) + np;
     q.n_items = (long long)(pl->chunk.items.size() - np);
     if (q.n_items > 0) {
-      err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], e->stream)
-                : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], e->stream);
+      err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], pl->stream)
+                : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "primary tier launch");
       ++n;
     }
-    VD_CUDA(cudaEventRecordWithFlags(e->ev_mid, e->stream, evflags));
+    VD_CUDA(cudaEventRecordWithFlags(pl->ev_mid, pl->stream, evflags));
     BatchView rv = bv;
     rv.hap_sel = nullptr;
     rv.out_sel = nullptr;
@@ -712,7 +784,7 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       q1.head = cnt + 1;
       q1.spill = (RescueEntry*)(d + L.o_sp2);
       q1.spill_count = cnt + 4;
-      err = launch_f64(anch, rv, q1, &dt->f64, ht->s64, 1, e->grid[1][anch], e->stream);
+      err = launch_f64(anch, rv, q1, &dt->f64, ht->s64, 1, e->grid[1][anch], pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "rescue tier launch");
       ++n;
     }
@@ -727,36 +799,48 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
     q2.spill_count = nullptr;
     q2.spill_cap = 0;
     const int robust_grid = pl->chunk.any_strip ? e->grid[1][anch] : std::min(e->grid[1][anch], kRobustBlocks);
-    err = launch_f64(anch, rv, q2, &dt->f64, ht->s64, 2, robust_grid, e->stream);
+    err = launch_f64(anch, rv, q2, &dt->f64, ht->s64, 2, robust_grid, pl->stream);
     if (err != cudaSuccess) return cuda_fail(err, "robust tier launch");
     ++n;
   } else {
-    VD_CUDA(cudaEventRecordWithFlags(e->ev_mid, e->stream, evflags));
+    VD_CUDA(cudaEventRecordWithFlags(pl->ev_mid, pl->stream, evflags));
   }
-  VD_CUDA(cudaEventRecordWithFlags(e->ev_end, e->stream, evflags));
+  VD_CUDA(cudaEventRecordWithFlags(pl->ev_end, pl->stream, evflags));
   if (launches) *launches = n;
   return VD_OK;
 }
 
-int tier_times(vd_engine* e, double* total, double* primary, double* rescue) {
+int tier_times(const vd_plan* pl, double* total, double* primary, double* rescue) {
   float a = 0.f, b = 0.f;
-  VD_CUDA(cudaEventElapsedTime(&a, e->ev_begin, e->ev_mid));
-  VD_CUDA(cudaEventElapsedTime(&b, e->ev_mid, e->ev_end));
+  VD_CUDA(cudaEventElapsedTime(&a, pl->ev_begin, pl->ev_mid));
+  VD_CUDA(cudaEventElapsedTime(&b, pl->ev_mid, pl->ev_end));
   *primary += a;
   *rescue += b;
   *total += a + b;
   return VD_OK;
 }
 
-int read_counters(vd_plan* pl, int64_t* r1, int64_t* r2) {
-  unsigned long long h[6];
-  VD_CUDA(cudaMemcpyAsync(h, pl->base + pl->L.o_cnt, sizeof(h), cudaMemcpyDeviceToHost, pl->eng->stream));
-  VD_CUDA(cudaStreamSynchronize(pl->eng->stream));
+int enqueue_counter_read(vd_plan* pl, unsigned long long* host) {
+  VD_CUDA(cudaMemcpyAsync(host, pl->base + pl->L.o_cnt, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          pl->stream));
+  return VD_OK;
+}
+
+// after the plan's stream completed
+int check_counters(const vd_plan* pl, const unsigned long long* h, int64_t* r1, int64_t* r2) {
   if (h[5]) return fail(VD_EOVERFLOW, "rescue list overflow");
   const bool f64 = pl->params.precision == VD_PRECISION_FLOAT64;
   *r1 = f64 ? 0 : (int64_t)h[3];
   *r2 = (int64_t)(f64 ? h[3] : h[4]);
   return VD_OK;
+}
+
+int read_counters(vd_plan* pl, int64_t* r1, int64_t* r2) {
+  unsigned long long h[6];
+  int rc = enqueue_counter_read(pl, h);
+  if (rc) return rc;
+  VD_CUDA(cudaStreamSynchronize(pl->stream));
+  return check_counters(pl, h, r1, r2);
 }
 
 int init_engine_grids(vd_engine* e) {
@@ -844,6 +928,14 @@ int vd_engine_create(int device, int64_t memory_mb, vd_engine** out) {
       (err = cudaMallocHost((void**)&e->htab, sizeof(TableSet))) != cudaSuccess) {
     rc = cuda_fail(err, "engine setup");
   }
+  for (int k = 0; k < 2 && !rc; ++k) {
+    vd_engine::Slot& sl = e->slots[k];
+    if ((err = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (err = cudaEventCreate(&sl.ev[0])) != cudaSuccess || (err = cudaEventCreate(&sl.ev[1])) != cudaSuccess ||
+        (err = cudaEventCreate(&sl.ev[2])) != cudaSuccess ||
+        (err = cudaMallocHost((void**)&sl.hcnt, 16 * sizeof(unsigned long long))) != cudaSuccess)
+      rc = cuda_fail(err, "engine pipeline setup");
+  }
   if (!rc) rc = init_engine_grids(e);
   if (rc) { vd_engine_destroy(e); return rc; }
   *out = e;
@@ -864,6 +956,15 @@ int vd_engine_destroy(vd_engine* e) {
       pl->eng = nullptr;
     }
     e->plans.clear();
+    for (vd_engine::Slot& sl : e->slots) {
+      if (sl.stream) cudaStreamSynchronize(sl.stream);
+      delete sl.pl;
+      sl.pl = nullptr;
+      sl.arena.release();
+      for (cudaEvent_t& ev : sl.ev) if (ev) cudaEventDestroy(ev);
+      if (sl.hcnt) cudaFreeHost(sl.hcnt);
+      if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
     e->arena.release();
     e->dtab.release();
     if (e->htab) cudaFreeHost(e->htab);
@@ -926,6 +1027,20 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     return 2 * (b->read_off[r1] - b->read_off[r0]) + (r1 - r0) * 64 + (b->hap_off[h1] - b->hap_off[h0]) +
            (h1 - h0) * 8 + np * (8 + 32);
   };
+  // DP cells per unit: large batches are cut into several chunks so that the
+  // host work of one chunk overlaps the kernels of the previous one
+  auto unit_cells = [&](int64_t u) -> int64_t {
+    if (pair_form) return (b->read_off[u + 1] - b->read_off[u]) * 512 * (pg.start[u + 1] - pg.start[u]);
+    const int64_t r0 = b->region_read_off[u], r1 = b->region_read_off[u + 1];
+    const int64_t h0 = b->region_hap_off[u], h1 = b->region_hap_off[u + 1];
+    return (b->read_off[r1] - b->read_off[r0]) * (b->hap_off[h1] - b->hap_off[h0]);
+  };
+  int64_t total_cells = 0;
+  for (int64_t u = 0; u < units; ++u) total_cells += unit_cells(u);
+  constexpr int64_t kPipelineCells = 150'000'000'000LL;  // ~50 ms of kernel time per chunk
+  const int64_t n_pipe = std::max<int64_t>(1, std::min<int64_t>(8, total_cells / kPipelineCells));
+  const int64_t chunk_cells = n_pipe > 1 ? (total_cells + n_pipe - 1) / n_pipe : INT64_MAX;
+
   int64_t fixed = pair_form ? (b->hap_off[b->n_haps] - b->hap_off[0]) + 8 * b->n_haps : 0;
   int64_t max_hap = 0, max_read = 0;
   for (int64_t h = 0; h < b->n_haps; ++h) max_hap = std::max<int64_t>(max_hap, b->hap_off[h + 1] - b->hap_off[h]);
@@ -933,57 +1048,80 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   const int64_t scratch_warps = max_read + p->anchored > kStripRows ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
   fixed += (max_hap + 1) * scratch_warps * (int64_t)sizeof(double2) + 64 * 1024;
   const int64_t budget = (int64_t)e->budget;
-  int64_t u = 0;
-  std::vector<double>& stage = e->out_stage;
-  int64_t region_out_base = 0;
+
+  // results of the chunk in a slot, once its stream has completed
+  auto finish = [&](vd_engine::Slot& sl) -> int {
+    if (!sl.busy) return VD_OK;
+    sl.busy = false;
+    VD_CUDA(cudaStreamSynchronize(sl.stream));
+    vd_plan& pl = *sl.pl;
+    int64_t r1 = 0, r2 = 0;
+    int r = check_counters(&pl, sl.hcnt, &r1, &r2);
+    if (r) return r;
+    if ((r = tier_times(&pl, &s.kernel_ms, &s.primary_ms, &s.rescue_ms))) return r;
+    s.rescued_fp64 += r1;
+    s.rescued_robust += r2;
+    const HostChunk& c = pl.chunk;
+    if (pair_form) for (int64_t k = 0; k < c.n_out; ++k) out[c.out_global[k]] = sl.stage[k];
+    return VD_OK;
+  };
+
+  int64_t u = 0, chunk_index = 0;
   while (u < units) {
-    int64_t u_end = u, bytes = fixed;
+    int64_t u_end = u, bytes = fixed, cells = 0;
     while (u_end < units) {
       const int64_t ub = unit_bytes(u_end);
-      if (u_end > u && bytes + ub > budget) break;
+      if (u_end > u && (bytes + ub > budget || cells >= chunk_cells)) break;
       bytes += ub;
+      cells += unit_cells(u_end);
       ++u_end;
     }
     if (bytes > budget) return fail(VD_ENOMEM, "One pair exceeds CUDA workspace budget");
-    const double th = now_ms();
-    vd_plan pl;
+    vd_engine::Slot& sl = e->slots[chunk_index & 1];
+    if ((rc = finish(sl))) return rc;  // the slot's previous chunk
+    if (!sl.pl) sl.pl = new vd_plan();
+    vd_plan& pl = *sl.pl;
+    pl.chunk = HostChunk();
     pl.eng = e;
     pl.params = *p;
+    pl.stream = sl.stream;
+    pl.ev_begin = sl.ev[0];
+    pl.ev_mid = sl.ev[1];
+    pl.ev_end = sl.ev[2];
+    const double th = now_ms();
     if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk);
     else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED, pl.chunk);
     HostChunk& c = pl.chunk;
     pl.L = layout_for(c, b, warps);
     s.host_ms += now_ms() - th;
-    if ((rc = e->arena.reserve(pl.L.total))) return rc;
-    pl.base = (char*)e->arena.p;
-    s.live_bytes = std::max<int64_t>(s.live_bytes, (int64_t)pl.L.total);
+    if ((rc = sl.arena.reserve(pl.L.total))) return rc;
+    pl.base = (char*)sl.arena.p;
+    s.live_bytes = std::max<int64_t>(s.live_bytes, (int64_t)(e->slots[0].arena.bytes + e->slots[1].arena.bytes));
     if ((rc = upload_chunk(&pl, b, &s.h2d_bytes))) return rc;
     int launches = 0;
     if ((rc = enqueue_tiers(&pl, &launches))) return rc;
     s.kernel_launches += launches + (c.n_out > 0 ? 1 : 0);  // the -inf fill of the upload
-    // results
     const double* dout = (const double*)(pl.base + pl.L.o_out);
     if (c.n_out > 0) {
       if (pair_form) {
-        stage.resize((size_t)c.n_out);
-        VD_CUDA(cudaMemcpyAsync(stage.data(), dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        sl.stage.resize((size_t)c.n_out);
+        VD_CUDA(cudaMemcpyAsync(sl.stage.data(), dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, sl.stream));
       } else {
-        VD_CUDA(cudaMemcpyAsync(out + c.out_begin, dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        VD_CUDA(cudaMemcpyAsync(out + c.out_begin, dout, (size_t)c.n_out * sizeof(double), cudaMemcpyDeviceToHost, sl.stream));
       }
       s.d2h_bytes += c.n_out * (int64_t)sizeof(double);
     }
-    int64_t r1 = 0, r2 = 0;
-    if ((rc = read_counters(&pl, &r1, &r2))) return rc;
-    if ((rc = tier_times(e, &s.kernel_ms, &s.primary_ms, &s.rescue_ms))) return rc;
-    s.rescued_fp64 += r1;
-    s.rescued_robust += r2;
-    if (pair_form) for (int64_t k = 0; k < c.n_out; ++k) out[c.out_global[k]] = stage[k];
+    if ((rc = enqueue_counter_read(&pl, sl.hcnt))) return rc;
+    sl.busy = true;
     s.dp_cells += c.cells;
     s.work_items += (int64_t)c.items.size();
     ++s.batches;
-    region_out_base += c.n_out;
+    ++chunk_index;
     u = u_end;
   }
+  // drain in submission order
+  if ((rc = finish(e->slots[chunk_index & 1]))) return rc;
+  if ((rc = finish(e->slots[(chunk_index + 1) & 1]))) return rc;
   s.total_ms = now_ms() - t0;
   if (st) *st = s;
   return VD_OK;
@@ -1001,6 +1139,10 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
   vd_plan* pl = new vd_plan();
   pl->eng = e;
   pl->params = *p;
+  pl->stream = e->stream;
+  pl->ev_begin = e->ev_begin;
+  pl->ev_mid = e->ev_mid;
+  pl->ev_end = e->ev_end;
   if (p->quality_offsets) {
     pl->has_offsets = true;
     for (int i = 0; i < 4; ++i) pl->offsets[i] = p->quality_offsets[i];
@@ -1054,7 +1196,7 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
   int64_t r1 = 0, r2 = 0;
   if ((rc = read_counters(pl, &r1, &r2))) return rc;
   double ms = 0.0, pms = 0.0, rms = 0.0;
-  if ((rc = tier_times(e, &ms, &pms, &rms))) return rc;
+  if ((rc = tier_times(pl, &ms, &pms, &rms))) return rc;
   pl->last_rescued1 = r1;
   pl->last_rescued2 = r2;
   if (st) {
