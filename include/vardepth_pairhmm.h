@@ -7,8 +7,9 @@
  * reference's C ABI (caller/native/caller/batch_hmm.cpp:217-219,
  * trie_vector.cpp:284-286): 0 = OK, 1 = bad arguments; codes >= 2 are device
  * errors this library adds.  vd_last_error() describes the last failure of
- * the calling thread.  All inputs are caller-owned host memory; nothing is
- * retained after a call returns (plans excepted, see below).
+ * the calling thread.  All inputs are caller-owned host memory (device memory
+ * for vd_forward_region_noalloc); nothing is retained after a call returns
+ * (plans excepted, see below).
  */
 #ifndef VARDEPTH_PAIRHMM_H
 #define VARDEPTH_PAIRHMM_H
@@ -151,6 +152,34 @@ double vd_read_haplotype(const char *read, const unsigned char *qual, int n, con
                          double gap, double ext);
 double vd_anchored_pairhmm(const char *read, const unsigned char *qual, int n, const char *hap,
                            int m, double gap, double ext);
+
+/* ---- a call that allocates nothing ----------------------------------------
+ * No counterpart in the reference.  For callers that may not call cudaMalloc
+ * or any allocating routine: code running under a framework's caching
+ * allocator or a fixed memory pool that must not be bypassed, processes that
+ * forbid driver allocations after start-up, and code that must not block on
+ * the allocator.  Scores one region -- every read against every haplotype,
+ * out[r * n_haps + h] -- whose inputs (packed as in vd_batch) and output the
+ * caller holds in DEVICE memory of `device`, enqueued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream), and waits for that stream
+ * before returning.
+ *
+ * All scratch (counters, work codes, rescue lists, strip boundaries, model
+ * tables) is one fixed static device array of about 8 MiB, which every GPU that
+ * loads this library holds until the process exits.  Limits per call: at most
+ * 131072 reads, 4096 haplotypes and 131072 read x haplotype pairs, reads of at
+ * most 255 bases and haplotypes of at most 1023 bases; larger regions are
+ * rejected with VD_EINVAL (split them).  The first call on a device looks up
+ * the array's device address and the grid sizes, so make that first call
+ * before any stream capture.  Every call shares the one array (the previous
+ * call's contents stay in it; each call clears what must start at zero), so
+ * overlapping calls would race on it and must not happen; calls from several
+ * host threads of one process are serialised by a lock. */
+int vd_forward_region_noalloc(int device, const unsigned char *read_bases,
+                              const unsigned char *read_quals, const int64_t *read_off,
+                              int64_t n_reads, const unsigned char *hap_bases,
+                              const int64_t *hap_off, int64_t n_haps, const vd_params *params,
+                              double *out, void *stream);
 
 /* ---- misc ---------------------------------------------------------------- */
 const char *vd_last_error(void);

@@ -61,3 +61,19 @@ def test_engine_argument_errors(built_library):
     assert lib.vd_pairhmm_pairs(None, None, None, None, None, 1, 3, 0, None) == 1
     assert lib.vd_trie_many(None, None, None, -1, None, None, 0, 0, 0, None, None) == 1
     assert lib.vd_pairhmm_pairs(None, None, None, None, None, 0, 0, 0, None) == 0
+
+
+def test_noalloc_limits_are_checked_on_the_host(built_library):
+    from vardepth_b200 import native
+    lib = native.library()
+    params, _keep = native.make_params(0.001, 0.1, False, native.VD_PRECISION_MIXED)
+    # 1024 reads x 1024 haplotypes is beyond the 131072-pair scratch: rejected before any CUDA call
+    assert lib.vd_forward_region_noalloc(0, 1, 1, 1, 1024, 1, 1, 1024, ctypes.byref(params), 1, None) \
+        == native.VD_EINVAL
+    assert b"split the region" in lib.vd_last_error()
+    assert lib.vd_forward_region_noalloc(0, None, None, None, 0, None, None, 0, None, None, None) \
+        == native.VD_EINVAL
+    if lib.vd_device_count() == 0:
+        # a valid request with no GPU fails loudly instead of computing on the CPU
+        assert lib.vd_forward_region_noalloc(0, 1, 1, 1, 4, 1, 1, 4, ctypes.byref(params), 1, None) \
+            == native.VD_ENODEV

@@ -33,6 +33,7 @@ UNITS = [
     ("launch", "pairhmm_launch.cu", []),
     ("host", "pairhmm_host.cu", []),
     ("peak", "pairhmm_peak.cu", []),
+    ("noalloc", "pairhmm_noalloc.cu", []),
 ]
 
 

@@ -887,6 +887,24 @@ int default_precision() {
 
 }  // namespace
 
+namespace vd {
+// Records the calling thread's error for vd_last_error (used by the other
+// translation units of the library) and returns the code.
+int report_error(int code, const char* msg) { return fail(code, msg); }
+
+// The model tables of one (gap, ext, offsets) setting for callers outside this
+// file (the no-allocation entry point builds them into its own buffers).
+void build_model_tables(double gap, double ext, const double* offsets, Tables<float>* f32, Tables<double>* f64,
+                        Scalars<float>* s32, Scalars<double>* s64) {
+  static TableSet ts;  // 40 KB; callers serialise on their own lock
+  build_tables(gap, ext, offsets, &ts);
+  *f32 = ts.f32;
+  *f64 = ts.f64;
+  *s32 = ts.s32;
+  *s64 = ts.s64;
+}
+}  // namespace vd
+
 extern "C" {
 
 const char* vd_last_error(void) { return g_last_error.c_str(); }

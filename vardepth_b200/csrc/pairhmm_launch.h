@@ -14,4 +14,9 @@ cudaError_t occupancy_f64(bool anchored, int* blocks_per_sm);
 cudaError_t launch_pair_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                             const Scalars<float>& sc, int grid, cudaStream_t stream);
 cudaError_t occupancy_pair_f32(int* blocks_per_sm);
+// sets the message vd_last_error returns on this thread; returns code
+int report_error(int code, const char* msg);
+// model tables for (gap, ext, optional per-bin Phred offsets), built on the host
+void build_model_tables(double gap, double ext, const double* offsets, Tables<float>* f32, Tables<double>* f64,
+                        Scalars<float>* s32, Scalars<double>* s64);
 }  // namespace vd

@@ -79,6 +79,10 @@ SIGNATURES = {
                                             ctypes.c_double, ctypes.c_double]),
     "vd_anchored_pairhmm": (ctypes.c_double, [ctypes.c_char_p, c_u8p, ctypes.c_int, ctypes.c_char_p,
                                               ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+    # device pointers in and out; scratch in a fixed static device array
+    "vd_forward_region_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 c_i64, ctypes.c_void_p, ctypes.c_void_p, c_i64,
+                                                 ctypes.POINTER(VdParams), ctypes.c_void_p, ctypes.c_void_p]),
     "vd_last_error": (ctypes.c_char_p, []),
     "vd_device_count": (ctypes.c_int, []),
     "vd_version": (ctypes.c_char_p, []),
