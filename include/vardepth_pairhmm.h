@@ -34,6 +34,17 @@ enum {
   VD_PRECISION_FLOAT64 = 1  /* every pair in the FP64 wavefront */
 };
 
+/* How the primary tier assigns pairs to warps. */
+enum {
+  VD_SCHEDULE_BATCHED = 0,  /* persistent warps on a work queue; one item streams a read through
+                               all haplotypes of its region; items grouped by read length (rows
+                               per lane) and ordered longest first; two reads per warp where
+                               possible */
+  VD_SCHEDULE_PLAIN = 1     /* the comparison baseline: one read x haplotype pair per item, a
+                               fixed tile of 8 rows per lane, items in input order, assigned
+                               round-robin to a fixed grid of warps (no queue, no binning) */
+};
+
 /* Model parameters of one call. */
 typedef struct vd_params {
   double gap;       /* gap-open probability g (reference production value 0.001) */
@@ -43,7 +54,8 @@ typedef struct vd_params {
   const double *quality_offsets; /* NULL, or 4 Phred offsets added per quality bin
                                     (bins: q<15, q<25, q<35, q>=35); no counterpart in
                                     the reference, NULL reproduces it exactly */
-  int reserved[4];  /* must be zero */
+  int schedule;     /* VD_SCHEDULE_* (0 = batched) */
+  int reserved[3];  /* must be zero */
 } vd_params;
 
 /* A batch of reads and haplotypes in packed buffers.  Read r occupies

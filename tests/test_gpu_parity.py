@@ -240,6 +240,30 @@ def test_plan_graph_replay_is_deterministic():
         np.testing.assert_array_equal(o, ref)
 
 
+@pytest.mark.parametrize("anchored", [False, True])
+@pytest.mark.parametrize("precision", [native.VD_PRECISION_MIXED, native.VD_PRECISION_FLOAT64])
+def test_plain_schedule_gives_identical_results(anchored, precision):
+    """VD_SCHEDULE_PLAIN (one pair per item, fixed 8 rows per lane, input order) runs the same
+    arithmetic as the batched schedule, so every pair agrees bit for bit; long reads included."""
+    w = S.config1(n_regions=40)
+    eng = native.Engine(0, 4096)
+    batched, _ = native.make_params(w.gap, w.ext, anchored, precision)
+    plain, _ = native.make_params(w.gap, w.ext, anchored, precision, schedule=native.VD_SCHEDULE_PLAIN)
+    a, st_a = eng.forward(_packed(w), batched)
+    b, st_b = eng.forward(_packed(w), plain)
+    np.testing.assert_array_equal(a, b)
+    assert st_b.work_items == w.pairs() > st_a.work_items
+    pr, ph = w.explicit_pairs()
+    pairs_form = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
+                               pair_read=pr, pair_hap=ph)
+    np.testing.assert_array_equal(eng.forward(pairs_form, plain)[0], a)
+    plan = eng.plan(_packed(w), plain)
+    plan.run()
+    np.testing.assert_array_equal(plan.fetch(), a)
+    plan.close()
+    eng.close()
+
+
 def test_reference_shaped_entry_points():
     """The C-ABI drop-ins for pairhmm_pairs / trie_many / read_haplotype_batch_mode / read_haplotype."""
     lib = native.library()

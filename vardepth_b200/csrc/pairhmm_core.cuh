@@ -114,6 +114,7 @@ struct QueueView {
   void* scratch;              // strip boundaries: per warp slot, scratch_stride elements
   long long scratch_stride;   // in boundary records (float2 / double2)
   int* error_flag;            // set when the spill list overflows
+  int static_order;           // 1: warp w takes items w, w + W, w + 2W ... (W = warps in the grid)
 };
 
 }  // namespace vd

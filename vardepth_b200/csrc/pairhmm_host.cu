@@ -229,7 +229,9 @@ int validate_params(const vd_params* p) {
   if (p->quality_offsets)
     for (int i = 0; i < 4; ++i)
       if (!std::isfinite(p->quality_offsets[i])) return fail(VD_EINVAL, "quality offsets must be finite");
-  for (int i = 0; i < 4; ++i) if (p->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  if (p->schedule != VD_SCHEDULE_BATCHED && p->schedule != VD_SCHEDULE_PLAIN)
+    return fail(VD_EINVAL, "unknown schedule");
+  for (int i = 0; i < 3; ++i) if (p->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
   return VD_OK;
 }
 
@@ -420,8 +422,12 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
 // haplotype (their strip boundary scratch holds one haplotype).  With
 // pair_reads, two reads of a region with the same kernel variant (single strip,
 // one-sided emission) share an item and run in the packed two-read path.
+// With plain (the comparison schedule) every pair is its own item with the
+// fixed tile of kMaxR rows per lane, the list stays in input order and no
+// reads are paired.
 void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSet* ts, bool offsets,
-                        bool anchored, bool pair_reads, HostChunk& c) {
+                        bool anchored, bool pair_reads, HostChunk& c, bool plain = false) {
+  if (plain) pair_reads = false;
   c.ra = b->region_read_off[g0];
   c.rb = b->region_read_off[g1];
   c.ha = b->region_hap_off[g0];
@@ -461,7 +467,8 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       const int32_t code = c.read_code[r - c.ra];
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
       const int n2 = r2 >= 0 ? (int)(c.read_off[r2 - c.ra + 1] - c.read_off[r2 - c.ra]) : 0;
-      const int R = code_R(code);
+      const int R = plain ? kMaxR : code_R(code);
+      const int item_code = plain ? (code & ~15) | kMaxR : code;
       const int n_rows = n + (anchored ? 1 : 0);
       const int64_t rows = (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R));
       const bool multistrip = n_rows > kStripRows;
@@ -473,7 +480,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
         while (run_end < h_hi) {
           const int m = (int)(b->hap_off[run_end + 1] - b->hap_off[run_end]);
           if (m <= 0) break;
-          if (run_end > h && (multistrip || stream + m + 1 > kMaxStream)) break;
+          if (run_end > h && (plain || multistrip || stream + m + 1 > kMaxStream)) break;
           stream += m + 1;
           sl.cells += (int64_t)(n + n2) * m;
           sl.pairs += r2 >= 0 ? 2 : 1;
@@ -484,7 +491,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
         w.nhap = (int32_t)(run_end - h);
         w.hap_begin = h - c.ha;
         w.out_begin = region_out + (r - r_lo) * nh + (h - h_lo);
-        w.code = r2 >= 0 ? (code | kPairedBit) : code;
+        w.code = r2 >= 0 ? (item_code | kPairedBit) : item_code;
         w.read2 = r2 >= 0 ? (int32_t)(r2 - c.ra) : -1;
         w.out2_begin = r2 >= 0 ? region_out + (r2 - r_lo) * nh + (h - h_lo) : 0;
         items.push_back(w);
@@ -526,7 +533,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   }
   const int64_t out = region_out_of[ng];
   c.n_out = out;
-  order_items(c.items, cost);
+  if (!plain) order_items(c.items, cost);
   auto mid = std::stable_partition(c.items.begin(), c.items.end(),
                                    [](const WorkItem& w) { return code_paired(w.code); });
   c.n_paired = (int64_t)(mid - c.items.begin());
@@ -549,7 +556,7 @@ void group_pairs(const vd_batch* b, PairGroups& pg) {
 }
 
 void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64_t rb, const TableSet* ts,
-                      bool offsets, bool anchored, HostChunk& c) {
+                      bool offsets, bool anchored, HostChunk& c, bool plain = false) {
   c.ra = ra;
   c.rb = rb;
   c.ha = 0;
@@ -558,11 +565,11 @@ void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64
   std::vector<int64_t> cost;
   const int kMaxStream = 1 << 30;
   for (int64_t r = ra; r < rb; ++r) {
-    const int32_t code = c.read_code[r - ra];
+    const int32_t code = plain ? (c.read_code[r - ra] & ~15) | kMaxR : c.read_code[r - ra];
     const int n = (int)(c.read_off[r - ra + 1] - c.read_off[r - ra]);
     const int R = code_R(code);
     const int n_rows = n + (anchored ? 1 : 0);
-    const bool multistrip = n_rows > kStripRows;
+    const bool multistrip = plain || n_rows > kStripRows;
     const int64_t rows = n > 0 ? (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R)) : 0;
     int64_t list_begin = (int64_t)c.hap_sel.size();
     int64_t stream = 0;
@@ -602,7 +609,7 @@ void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64
     flush();
   }
   c.n_out = (int64_t)c.out_global.size();
-  order_items(c.items, cost);
+  if (!plain) order_items(c.items, cost);
 }
 
 // Device bytes a chunk needs (inputs, lists, outputs, rescue lists, scratch).
@@ -764,6 +771,7 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
     }
     q.items = (const WorkItem*)(d + L.o_items) + np;
     q.n_items = (long long)(pl->chunk.items.size() - np);
+    q.static_order = pl->params.schedule == VD_SCHEDULE_PLAIN ? 1 : 0;
     if (q.n_items > 0) {
       err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], pl->stream)
                 : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], pl->stream);
@@ -774,6 +782,7 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
     BatchView rv = bv;
     rv.hap_sel = nullptr;
     rv.out_sel = nullptr;
+    q.static_order = 0;  // the rescue tiers always run on the shared counter
     QueueView q1 = q;
     if (!f64) {
       // tier 1: FP64 wavefront over the FP32 spills
@@ -1107,8 +1116,10 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     pl.ev_mid = sl.ev[1];
     pl.ev_end = sl.ev[2];
     const double th = now_ms();
-    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk);
-    else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED, pl.chunk);
+    const bool plain = p->schedule == VD_SCHEDULE_PLAIN;
+    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk, plain);
+    else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED,
+                            pl.chunk, plain);
     HostChunk& c = pl.chunk;
     pl.L = layout_for(c, b, warps);
     s.host_ms += now_ms() - th;
@@ -1167,12 +1178,14 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
     pl->params.quality_offsets = pl->offsets;
   }
   const bool offsets = p->quality_offsets != nullptr;
+  const bool plain = p->schedule == VD_SCHEDULE_PLAIN;
   if (b->pair_read) {
     PairGroups pg;
     group_pairs(b, pg);
-    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, p->anchored != 0, pl->chunk);
+    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, p->anchored != 0, pl->chunk, plain);
   } else {
-    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED, pl->chunk);
+    build_region_chunk(b, 0, b->n_regions, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED,
+                       pl->chunk, plain);
   }
   pl->L = layout_for(pl->chunk, b, max_grid_warps(e));
   if ((rc = pl->own.reserve(pl->L.total))) { delete pl; return rc; }

@@ -641,10 +641,19 @@ pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restri
     const long long c = (long long)*qv.count;
     total = c < total ? c : total;
   }
+  // the plain schedule walks the list in a fixed round-robin order; the
+  // batched one pulls items from the shared counter
+  const long long stride = (long long)gridDim.x * kWarpsPerBlock;
+  long long next = gw;
   for (;;) {
     unsigned long long i = 0;
-    if (lane == 0) i = atomicAdd(qv.head, 1ull);
-    i = __shfl_sync(0xffffffffu, i, 0);
+    if (qv.static_order) {
+      i = (unsigned long long)next;
+      next += stride;
+    } else {
+      if (lane == 0) i = atomicAdd(qv.head, 1ull);
+      i = __shfl_sync(0xffffffffu, i, 0);
+    }
     if ((long long)i >= total) break;
     ItemRef it;
     it.tier = tier;

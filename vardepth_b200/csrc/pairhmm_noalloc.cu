@@ -253,7 +253,9 @@ extern "C" int vd_forward_region_noalloc(int device, const unsigned char* read_b
       (params->anchored != 0 && params->anchored != 1) ||
       (params->precision != VD_PRECISION_MIXED && params->precision != VD_PRECISION_FLOAT64))
     return na_fail(VD_EINVAL, "invalid params (gap in [0,0.5), ext in [0,1), anchored 0/1, known precision)");
-  for (int i = 0; i < 4; ++i)
+  if (params->schedule != VD_SCHEDULE_BATCHED)
+    return na_fail(VD_EINVAL, "this call runs the batched schedule only (schedule must be 0)");
+  for (int i = 0; i < 3; ++i)
     if (params->reserved[i]) return na_fail(VD_EINVAL, "reserved fields must be zero");
   if (params->quality_offsets)
     for (int i = 0; i < 4; ++i)

@@ -18,6 +18,7 @@ LIB_PATH = HERE / "libvardepth_pairhmm.so"
 
 VD_OK, VD_EINVAL, VD_ECUDA, VD_ENODEV, VD_ENOMEM, VD_EOVERFLOW = range(6)
 VD_PRECISION_MIXED, VD_PRECISION_FLOAT64 = 0, 1
+VD_SCHEDULE_BATCHED, VD_SCHEDULE_PLAIN = 0, 1
 
 c_i64 = ctypes.c_int64
 c_i32 = ctypes.c_int32
@@ -29,7 +30,8 @@ c_dp = ctypes.POINTER(ctypes.c_double)
 
 class VdParams(ctypes.Structure):
     _fields_ = [("gap", ctypes.c_double), ("ext", ctypes.c_double), ("anchored", ctypes.c_int),
-                ("precision", ctypes.c_int), ("quality_offsets", c_dp), ("reserved", ctypes.c_int * 4)]
+                ("precision", ctypes.c_int), ("quality_offsets", c_dp), ("schedule", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
 
 
 class VdBatch(ctypes.Structure):
@@ -178,12 +180,14 @@ class Packed:
         return int(np.sum(rr * hh))
 
 
-def make_params(gap: float, ext: float, anchored: bool, precision: int, quality_offsets=None):
+def make_params(gap: float, ext: float, anchored: bool, precision: int, quality_offsets=None,
+                schedule: int = VD_SCHEDULE_BATCHED):
     p = VdParams()
     p.gap = float(gap)
     p.ext = float(ext)
     p.anchored = 1 if anchored else 0
     p.precision = int(precision)
+    p.schedule = int(schedule)
     keep = None
     if quality_offsets is not None:
         keep = np.ascontiguousarray(quality_offsets, dtype=np.float64)
