@@ -165,6 +165,39 @@ double vd_read_haplotype(const char *read, const unsigned char *qual, int n, con
 double vd_anchored_pairhmm(const char *read, const unsigned char *qual, int n, const char *hap,
                            int m, double gap, double ext);
 
+/* ---- gradient --------------------------------------------------------------
+ * No counterpart in the reference (it has no differentiable PairHMM).  For the
+ * semiglobal model, every pair's ln L and its six partial derivatives
+ *   jac[6 o + k] = d ln L_o / d theta_k,
+ *   theta = (Qg, Qx, o0, o1, o2, o3):  gap = 10^(-Qg/10), ext = 10^(-Qx/10),
+ *   and o_b the Phred offset of quality bin b (the bins of vd_params), so
+ *   that the error of a base with Phred q in bin b is 10^(-max(0, min(q,60) + o_b)/10).
+ * The derivatives are taken at params (gap, ext, quality_offsets; NULL offsets
+ * = all 0) by a reverse-wavefront sweep over the DP (reverse-mode
+ * differentiation of the scaled forward recurrence): FP32 for every pair
+ * whose FP32 forward stays in range, FP64 for the rest (all pairs with
+ * precision = VD_PRECISION_FLOAT64).  Memory: VD_CHECKPOINT_SQRT keeps the
+ * warp state every ceil(sqrt(T)) anti-diagonals (T = m + 33) and replays one
+ * segment at a time; VD_CHECKPOINT_ALL keeps every anti-diagonal.  Both give
+ * identical results.  Reads of at most 256 bases; anchored = 0; gap, ext > 0.
+ * out_ln and out_jac (6 doubles per output) are host arrays in the output
+ * order of vd_forward.  Empty reads or haplotypes give -inf and a zero row. */
+enum { VD_CHECKPOINT_SQRT = 0, VD_CHECKPOINT_ALL = 1 };
+
+typedef struct vd_grad_stats {
+  int64_t pairs;           /* output slots */
+  int64_t dp_cells;        /* sum of n*m over non-empty pairs */
+  int64_t fp64_pairs;      /* pairs differentiated in the FP64 pass */
+  int64_t failed_pairs;    /* NaN results: the FP64 pass underflowed as well */
+  int64_t scratch_bytes;   /* device bytes of checkpoints and segment buffers */
+  int64_t kernel_launches;
+  double kernel_ms;        /* device time of the two passes (CUDA events) */
+  double total_ms;         /* host wall time of the call */
+} vd_grad_stats;
+
+int vd_forward_backward(vd_engine *engine, const vd_batch *batch, const vd_params *params, int checkpoint,
+                        double *out_ln, double *out_jac, vd_grad_stats *stats);
+
 /* ---- a call that allocates nothing ----------------------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc
  * or any allocating routine: code running under a framework's caching

@@ -54,6 +54,12 @@ def lib() -> ctypes.CDLL:
     L.vdo_forward_pairs.argtypes = [c_u8p, c_u8p, c_i64p, c_u8p, c_i64p, c_i32p, c_i32p, ctypes.c_int64,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, c_dp]
+    L.vdo_grad_ex.restype = ctypes.c_int
+    L.vdo_grad_ex.argtypes = [c_u8p, c_u8p, ctypes.c_int, c_u8p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_int, c_dp, c_dp, c_dp]
+    L.vdo_grad_pairs.restype = ctypes.c_int
+    L.vdo_grad_pairs.argtypes = [c_u8p, c_u8p, c_i64p, c_u8p, c_i64p, c_i32p, c_i32p, ctypes.c_int64,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_int, c_dp, ctypes.c_int, c_dp, c_dp]
     return L
 
 
@@ -100,6 +106,67 @@ def forward_pairs(read_bases, read_quals, read_off, hap_bases, hap_off, pair_rea
     if rc:
         raise RuntimeError("oracle batch failed")
     return out
+
+
+# ---- gradient checkers (theta = gap-open Phred, gap-continuation Phred, 4 bin offsets) ---------
+
+def phred_to_prob(q: float) -> float:
+    return float(10.0 ** (-q / 10.0))
+
+
+def prob_to_phred(p: float) -> float:
+    return float(-10.0 * np.log10(p))
+
+
+def grad(read, qual, hap, gap, ext, anchored=False, offsets=None):
+    """Expected-count (forward-backward) gradient of ln L for one pair, long double: (ln L, jac[6])."""
+    r, q, h = _bytes(read), _bytes(qual), _bytes(hap)
+    ln = ctypes.c_double()
+    jac = np.zeros(6, np.float64)
+    off = None if offsets is None else np.ascontiguousarray(offsets, np.float64)
+    rc = lib().vdo_grad_ex(_p(r), _p(q), len(r), _p(h), len(h), gap, ext, int(anchored),
+                           None if off is None else off.ctypes.data_as(c_dp), ctypes.byref(ln),
+                           jac.ctypes.data_as(c_dp))
+    if rc:
+        raise MemoryError("oracle gradient: allocation failed")
+    return ln.value, jac
+
+
+def grad_pairs(read_bases, read_quals, read_off, hap_bases, hap_off, pair_read, pair_hap, gap, ext,
+               anchored=False, offsets=None, threads=0):
+    """grad() over explicit pairs of packed buffers, on host threads: (ln[P], jac[P, 6])."""
+    rb, rq, hb = _bytes(read_bases), _bytes(read_quals), _bytes(hap_bases)
+    ro = np.ascontiguousarray(read_off, np.int64)
+    ho = np.ascontiguousarray(hap_off, np.int64)
+    pr = np.ascontiguousarray(pair_read, np.int32)
+    ph = np.ascontiguousarray(pair_hap, np.int32)
+    ln = np.empty(len(pr), np.float64)
+    jac = np.empty((len(pr), 6), np.float64)
+    off = None if offsets is None else np.ascontiguousarray(offsets, np.float64)
+    rc = lib().vdo_grad_pairs(_p(rb), _p(rq), ro.ctypes.data_as(c_i64p), _p(hb), ho.ctypes.data_as(c_i64p),
+                              pr.ctypes.data_as(c_i32p), ph.ctypes.data_as(c_i32p), len(pr), gap, ext,
+                              int(anchored), None if off is None else off.ctypes.data_as(c_dp), int(threads),
+                              ln.ctypes.data_as(c_dp), jac.ctypes.data_as(c_dp))
+    if rc:
+        raise MemoryError("oracle gradient batch failed")
+    return ln, jac
+
+
+def fd_grad(read, qual, hap, theta, h=1e-3, anchored=False):
+    """Central finite differences (step h on every Phred-scale parameter) of the FP64 forward."""
+    theta = np.asarray(theta, np.float64)
+
+    def f(t):
+        return forward(read, qual, hap, phred_to_prob(t[0]), phred_to_prob(t[1]), anchored,
+                       SEMIGLOBAL_ROW_DIVIDE, offsets=t[2:6])
+
+    jac = np.empty(6)
+    for k in range(6):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        jac[k] = (f(tp) - f(tm)) / (2 * h)
+    return jac
 
 
 def region_pairs(region_read_off, region_hap_off):

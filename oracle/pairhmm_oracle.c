@@ -59,9 +59,12 @@ double vdo_forward_ld_ex(const unsigned char *read, const unsigned char *qual, i
                          const unsigned char *hap, int m, double gap, double ext,
                          int anchored, int clamp);
 
+/* Phred of a base after its bin offset is floored at 0 (an error rate of at
+ * most 1), as the library's tables do. */
 static double error_offset(unsigned q, const double *offsets) {
     if (!offsets) return error_of(q);
     double c = (double)(q < 60u ? q : 60u) + offsets[vdo_quality_bin(q)];
+    if (c < 0.0) c = 0.0;
     return pow(10.0, -c / 10.0);
 }
 
@@ -249,4 +252,163 @@ int vdo_forward_pairs(const unsigned char *bases, const unsigned char *quals,
     vdo_worker(&job);
     for (int t = 0; t < started; ++t) pthread_join(tid[t], NULL);
     return 0;
+}
+
+/* ---- gradient oracle --------------------------------------------------------
+ * d ln L / d theta for theta = (gap-open Phred Qg, gap-continuation Phred Qx,
+ * quality-bin offsets o0..o3), g = 10^(-Qg/10), x = 10^(-Qx/10),
+ * e_i = 10^(-max(0, min(q_i,60) + o_bin(q_i))/10).  The reference has no
+ * differentiable PairHMM; this is the forward-backward (expected-count)
+ * gradient of the model of wide.cpp:9-33 / anchored.cpp:5-25 in x87 long
+ * double without rescaling (exponent range to 2^-16382), for small cases:
+ *
+ *   alpha = the forward DP of vdo_forward_ex, beta = dZ/d(cell) (the adjoint
+ *   of every cell, accumulated in reverse topological order), and
+ *   dZ/dg = sum beta_M E (-2) M[i-1][j-1] + beta_I M[i-1][j]/4 + beta_D M[i][j-1]
+ *   dZ/dx = sum beta_M E (-1)(I+D)[i-1][j-1] + beta_I I[i-1][j]/4 + beta_D D[i][j-1]
+ *   dZ/de_i = sum_j beta_M[i][j] M[i][j] (match ? -1/(1-e) : 1/e)
+ *
+ * i.e. the expected transition counts times d ln(transition)/d theta.  The
+ * anchored 1e-300 floor of anchored.cpp:24 is not differentiated (where it
+ * binds, the value is a constant and its gradient would be 0). */
+int vdo_grad_ex(const unsigned char *read, const unsigned char *qual, int n,
+                const unsigned char *hap, int m, double gap, double ext, int anchored,
+                const double *offsets, double *ln_out, double *jac) {
+    for (int k = 0; k < 6; ++k) jac[k] = 0.0;
+    if (n <= 0 || m <= 0) { *ln_out = -INFINITY; return 0; }
+    const size_t W = (size_t)m + 1, N = ((size_t)n + 1) * W;
+    long double *buf = (long double *)calloc(6 * N + 2 * (size_t)n, sizeof(long double));
+    if (!buf) return 1;
+    long double *FM = buf, *FI = buf + N, *FD = buf + 2 * N;
+    long double *BM = buf + 3 * N, *BI = buf + 4 * N, *BD = buf + 5 * N;
+    long double *err = buf + 6 * N, *derr = err + n;  /* e_i and de_i / d o */
+    const long double G = gap, X = ext, a = 1.0L - 2.0L * G, b = 1.0L - X;
+    const long double L10 = logl(10.0L) / 10.0L;
+    for (int i = 0; i < n; ++i) {
+        unsigned q = qual[i];
+        long double ph = (long double)(q < 60u ? q : 60u) + (offsets ? offsets[vdo_quality_bin(q)] : 0.0);
+        /* at or below the Phred floor 0 the offset derivative is taken as 0 */
+        int clamped = ph <= 0.0L;
+        if (clamped) ph = 0.0L;
+        err[i] = powl(10.0L, -ph / 10.0L);
+        derr[i] = clamped ? 0.0L : -L10 * err[i];
+    }
+#define IX(i, j) ((size_t)(i) * W + (size_t)(j))
+#define EMIT(i, j) ((read[(i) - 1] == hap[(j) - 1]) ? 1.0L - err[(i) - 1] : err[(i) - 1] / 3.0L)
+    if (anchored) {
+        FM[IX(0, 0)] = 1.0L;
+        for (int j = 1; j <= m; ++j) FD[IX(0, j)] = G * FM[IX(0, j - 1)] + X * FD[IX(0, j - 1)];
+    } else {
+        for (int j = 0; j <= m; ++j) FM[IX(0, j)] = 1.0L / (long double)(m + 1);
+    }
+    for (int i = 1; i <= n; ++i) {
+        FI[IX(i, 0)] = 0.25L * (G * FM[IX(i - 1, 0)] + X * FI[IX(i - 1, 0)]);
+        for (int j = 1; j <= m; ++j) {
+            FM[IX(i, j)] = EMIT(i, j) * (a * FM[IX(i - 1, j - 1)] + b * (FI[IX(i - 1, j - 1)] + FD[IX(i - 1, j - 1)]));
+            FI[IX(i, j)] = 0.25L * (G * FM[IX(i - 1, j)] + X * FI[IX(i - 1, j)]);
+            FD[IX(i, j)] = G * FM[IX(i, j - 1)] + X * FD[IX(i, j - 1)];
+        }
+    }
+    long double Z = 0.0L;
+    if (anchored) {
+        Z = FM[IX(n, m)] + FI[IX(n, m)] + FD[IX(n, m)];
+        BM[IX(n, m)] = BI[IX(n, m)] = BD[IX(n, m)] = 1.0L;
+    } else {
+        for (int j = 0; j <= m; ++j) { Z += FM[IX(n, j)] + FI[IX(n, j)]; BM[IX(n, j)] = 1.0L; BI[IX(n, j)] = 1.0L; }
+    }
+    if (!(Z > 0.0L)) { free(buf); *ln_out = -INFINITY; return 0; }
+    long double dg = 0.0L, dx = 0.0L, dob[4] = {0.0L, 0.0L, 0.0L, 0.0L};
+    /* successors of (i,j) are (i+1,j+1), (i+1,j), (i,j+1): reverse row-major
+     * order completes every adjoint before it is propagated */
+    for (int i = n; i >= 0; --i) {
+        long double de = 0.0L;
+        for (int j = m; j >= 0; --j) {
+            const size_t c = IX(i, j);
+            if (i >= 1 && j >= 1) {
+                const long double E = EMIT(i, j), bm = BM[c];
+                const size_t p = IX(i - 1, j - 1);
+                BM[p] += bm * E * a;
+                BI[p] += bm * E * b;
+                BD[p] += bm * E * b;
+                dg += bm * E * (-2.0L) * FM[p];
+                dx += bm * E * (-1.0L) * (FI[p] + FD[p]);
+                const int match = read[i - 1] == hap[j - 1];
+                const long double e = err[i - 1];
+                if (derr[i - 1] != 0.0L) de += bm * FM[c] * (match ? -1.0L / (1.0L - e) : 1.0L / e);
+            }
+            if (i >= 1) {
+                const long double bi = BI[c];
+                const size_t p = IX(i - 1, j);
+                BM[p] += bi * 0.25L * G;
+                BI[p] += bi * 0.25L * X;
+                dg += bi * 0.25L * FM[p];
+                dx += bi * 0.25L * FI[p];
+            }
+            if (j >= 1 && (i >= 1 || anchored)) {
+                const long double bd = BD[c];
+                const size_t p = IX(i, j - 1);
+                BM[p] += bd * G;
+                BD[p] += bd * X;
+                dg += bd * FM[p];
+                dx += bd * FD[p];
+            }
+        }
+        if (i >= 1) dob[vdo_quality_bin(qual[i - 1])] += de * derr[i - 1];
+    }
+#undef IX
+#undef EMIT
+    jac[0] = (double)(dg / Z * (-L10 * G));
+    jac[1] = (double)(dx / Z * (-L10 * X));
+    for (int k = 0; k < 4; ++k) jac[2 + k] = (double)(dob[k] / Z);
+    *ln_out = (double)logl(Z);
+    free(buf);
+    return 0;
+}
+
+typedef struct {
+    const unsigned char *bases, *quals, *haps;
+    const int64_t *read_off, *hap_off;
+    const int32_t *pair_read, *pair_hap;
+    int64_t count, next;
+    double gap, ext;
+    int anchored;
+    const double *offsets;
+    double *ln, *jac;
+    int failed;
+} vdo_grad_job;
+
+static void *vdo_grad_worker(void *arg) {
+    vdo_grad_job *job = (vdo_grad_job *)arg;
+    for (;;) {
+        int64_t p = __atomic_fetch_add(&job->next, 1, __ATOMIC_RELAXED);
+        if (p >= job->count) break;
+        int32_t r = job->pair_read[p], h = job->pair_hap[p];
+        int n = (int)(job->read_off[r + 1] - job->read_off[r]);
+        int m = (int)(job->hap_off[h + 1] - job->hap_off[h]);
+        if (vdo_grad_ex(job->bases + job->read_off[r], job->quals + job->read_off[r], n,
+                        job->haps + job->hap_off[h], m, job->gap, job->ext, job->anchored, job->offsets,
+                        job->ln + p, job->jac + 6 * p))
+            __atomic_store_n(&job->failed, 1, __ATOMIC_RELAXED);
+    }
+    return NULL;
+}
+
+/* vdo_grad_ex over explicit pairs of packed buffers on `threads` host threads. */
+int vdo_grad_pairs(const unsigned char *bases, const unsigned char *quals, const int64_t *read_off,
+                   const unsigned char *haps, const int64_t *hap_off, const int32_t *pair_read,
+                   const int32_t *pair_hap, int64_t count, double gap, double ext, int anchored,
+                   const double *offsets, int threads, double *ln, double *jac) {
+    if (count < 0 || (count > 0 && (!ln || !jac))) return 1;
+    vdo_grad_job job = {bases, quals, haps, read_off, hap_off, pair_read, pair_hap, count, 0,
+                        gap, ext, anchored, offsets, ln, jac, 0};
+    if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    pthread_t tid[256];
+    int started = 0;
+    for (int t = 1; t < threads; ++t)
+        if (pthread_create(&tid[started], NULL, vdo_grad_worker, &job) == 0) ++started;
+    vdo_grad_worker(&job);
+    for (int t = 0; t < started; ++t) pthread_join(tid[t], NULL);
+    return job.failed;
 }

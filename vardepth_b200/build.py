@@ -34,6 +34,7 @@ UNITS = [
     ("host", "pairhmm_host.cu", []),
     ("peak", "pairhmm_peak.cu", []),
     ("noalloc", "pairhmm_noalloc.cu", []),
+    ("grad", "pairhmm_grad.cu", []),
 ]
 
 

@@ -27,6 +27,7 @@
 #include "../../include/vardepth_pairhmm.h"
 #include "pairhmm_core.cuh"
 #include "pairhmm_launch.h"
+#include "pairhmm_backward.cuh"
 
 using namespace vd;
 
@@ -171,6 +172,8 @@ struct vd_engine {
   std::mutex mu;
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair = 0;                  // blocks of the two-read kernel
+  int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
+  DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
   // table cache
   TableKey tkey{};
   bool tvalid = false;
@@ -647,6 +650,45 @@ Layout layout_for(const HostChunk& c, const vd_batch* b, int64_t warps) {
   return L;
 }
 
+// ---- gradient tables ---------------------------------------------------------------
+
+// Derivatives of the folded constants of build_tables with respect to the
+// Phred-scale parameters (Qg, Qx, bin offsets).  A quality whose Phred,
+// after its offset, is at or below the floor 0 has no offset derivative.
+void build_grad_tables(double g, double x, const double* offsets, GradTables* gt, GradScalars* gs) {
+  const double L10 = std::log(10.0) / 10.0;
+  for (int q = 0; q < 256; ++q) {
+    double ph = (double)std::min(q, 60) + (offsets ? offsets[quality_bin((unsigned)q)] : 0.0);
+    const bool floor = ph <= 0.0;
+    ph = std::max(0.0, ph);
+    const double e = std::pow(10.0, -ph / 10.0);
+    const double dE = floor ? 0.0 : -L10 * e;  // de / d offset
+    const double p1 = 1.0 - e, p0 = e / 3.0;
+    gt->bin[q] = quality_bin((unsigned)q);
+    if (dE == 0.0) {
+      gt->dlnN[q] = gt->dlnmiss[q] = gt->dlnhit[q] = 0.0;
+    } else if (p0 > p1) {  // two-sided rows: hit = 3(1-e)/e, miss = 1, N = a e/3
+      gt->dlnN[q] = dE / e;
+      gt->dlnmiss[q] = 0.0;
+      gt->dlnhit[q] = dE * (-1.0 / (1.0 - e) - 1.0 / e);
+    } else {               // hit = 1, miss = e/(3(1-e)), N = a (1-e)
+      gt->dlnN[q] = -dE / (1.0 - e);
+      gt->dlnmiss[q] = dE * (1.0 / e + 1.0 / (1.0 - e));
+      gt->dlnhit[q] = 0.0;
+    }
+  }
+  const double a = 1.0 - 2.0 * g, dg = -L10 * g, dx = -L10 * x;
+  gs->dlnN_g = (-2.0 / a) * dg;
+  gs->dlnK_g = (1.0 / g + 4.0 / a) * dg;
+  gs->dlnX_g = (2.0 / a) * dg;
+  gs->dlnA_g = (1.0 / g + 2.0 / a) * dg;
+  gs->dlnk2_g = (1.0 / g + 2.0 / a) * dg;
+  gs->dlnK_x = (-1.0 / (1.0 - x)) * dx;
+  gs->dlnX_x = (1.0 / x) * dx;
+  gs->dlnk2_x = (-1.0 / (1.0 - x)) * dx;
+  gs->dx_x = dx;
+}
+
 __global__ void fill_kernel(double* p, int64_t n, double v) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -864,6 +906,12 @@ int init_engine_grids(vd_engine* e) {
   cudaError_t err = occupancy_pair_f32(&bps);
   if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
   e->grid_pair = std::max(1, bps) * e->sm_count;
+  for (int f = 0; f < 2; ++f) {
+    bps = 0;
+    err = occupancy_grad(f != 0, &bps);
+    if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+    e->grid_grad[f] = std::max(1, bps) * e->sm_count;
+  }
   return VD_OK;
 }
 
@@ -993,6 +1041,7 @@ int vd_engine_destroy(vd_engine* e) {
       if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     e->arena.release();
+    e->grad_arena.release();
     e->dtab.release();
     if (e->htab) cudaFreeHost(e->htab);
     if (e->ev_begin) cudaEventDestroy(e->ev_begin);
@@ -1283,6 +1332,165 @@ int vd_plan_destroy(vd_plan* pl) {
     e->plans.erase(pl);
   }
   delete pl;
+  return VD_OK;
+}
+
+// ---- gradient -----------------------------------------------------------------------
+
+int vd_forward_backward(vd_engine* e, const vd_batch* b, const vd_params* p, int checkpoint, double* out_ln,
+                        double* out_jac, vd_grad_stats* st) {
+  const double t0 = now_ms();
+  if (!e) return fail(VD_EINVAL, "engine is NULL");
+  int rc = validate_params(p);
+  if (!rc) rc = validate_batch(b);
+  if (rc) return rc;
+  if (p->anchored) return fail(VD_EINVAL, "the gradient covers the semiglobal model (anchored = 0)");
+  if (p->schedule != VD_SCHEDULE_BATCHED) return fail(VD_EINVAL, "the gradient runs the batched schedule only");
+  if (!(p->gap > 0.0) || !(p->ext > 0.0)) return fail(VD_EINVAL, "the gradient needs gap > 0 and ext > 0");
+  if (checkpoint != VD_CHECKPOINT_SQRT && checkpoint != VD_CHECKPOINT_ALL) return fail(VD_EINVAL, "unknown checkpoint mode");
+  const int64_t n_out = batch_outputs(b);
+  if (n_out > 0 && (!out_ln || !out_jac)) return fail(VD_EINVAL, "out_ln or out_jac is NULL");
+  for (int64_t r = 0; r < b->n_reads; ++r)
+    if (b->read_off[r + 1] - b->read_off[r] > kStripRows)
+      return fail(VD_EINVAL, "the gradient supports reads of at most 256 bases");
+  std::lock_guard<std::mutex> lk(e->mu);
+  DeviceGuard guard(e->device);
+  vd_grad_stats s{};
+  s.pairs = n_out;
+  if ((rc = ensure_tables(e, p))) return rc;
+  const bool offsets = p->quality_offsets != nullptr;
+  const bool store_all = checkpoint == VD_CHECKPOINT_ALL;
+  const bool f64_only = p->precision == VD_PRECISION_FLOAT64;
+
+  // every input on the device once; reads carry the code of the forward tiers
+  HostChunk c;
+  c.ra = 0; c.rb = b->n_reads; c.ha = 0; c.hb = b->n_haps;
+  finish_chunk_common(c, b, e->htab, offsets, false);
+  std::vector<RescueEntry> items;
+  items.reserve((size_t)n_out);
+  std::vector<int64_t> empty_slots;
+  auto add = [&](int64_t r, int64_t h, int64_t o) {
+    const int64_t n = b->read_off[r + 1] - b->read_off[r], m = b->hap_off[h + 1] - b->hap_off[h];
+    if (n <= 0 || m <= 0) { empty_slots.push_back(o); return; }
+    items.push_back(RescueEntry{(int32_t)r, (int32_t)h, o});
+    s.dp_cells += n * m;
+  };
+  if (b->pair_read) {
+    for (int64_t q = 0; q < b->n_pairs; ++q) add(b->pair_read[q], b->pair_hap[q], q);
+  } else {
+    int64_t o = 0;
+    for (int64_t g = 0; g < b->n_regions; ++g)
+      for (int64_t r = b->region_read_off[g]; r < b->region_read_off[g + 1]; ++r)
+        for (int64_t h = b->region_hap_off[g]; h < b->region_hap_off[g + 1]; ++h) add(r, h, o++);
+  }
+  // group by kernel variant, longest haplotype first inside a group
+  auto hlen = [&](const RescueEntry& x) { return b->hap_off[x.hap + 1] - b->hap_off[x.hap]; };
+  std::stable_sort(items.begin(), items.end(), [&](const RescueEntry& x, const RescueEntry& y) {
+    const int cx = c.read_code[x.read] & 0x1ff, cy = c.read_code[y.read] & 0x1ff;
+    if (cx != cy) return cx > cy;
+    return hlen(x) > hlen(y);
+  });
+  long long slot_bytes = 256;
+  for (const RescueEntry& x : items)
+    slot_bytes = std::max(slot_bytes, grad_slot_bytes(code_R(c.read_code[x.read]), (int)hlen(x), store_all));
+  slot_bytes = (long long)align_up((size_t)slot_bytes, 256);
+  const int grid32 = e->grid_grad[0], grid64 = e->grid_grad[1];
+  const int64_t slots = (int64_t)std::max(grid32, grid64) * kWarpsPerBlock;
+
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + std::max<size_t>(bytes, 1), 256); return o; };
+  const int64_t read_bytes = c.read_off.back(), hap_bytes = c.hap_off.back();
+  const size_t o_rb = take(read_bytes), o_rq = take(read_bytes), o_roff = take(c.read_off.size() * 8),
+               o_rcode = take(c.read_code.size() * 4), o_hb = take(hap_bytes), o_hoff = take(c.hap_off.size() * 8),
+               o_items = take(items.size() * sizeof(RescueEntry)), o_spill = take(items.size() * sizeof(RescueEntry)),
+               o_ln = take((size_t)n_out * 8), o_jac = take((size_t)n_out * 48), o_cnt = take(8 * 8),
+               o_gt = take(sizeof(GradTables)), o_scratch = take((size_t)(slots * slot_bytes));
+  if ((rc = e->grad_arena.reserve(off))) return rc;
+  char* d = (char*)e->grad_arena.p;
+  s.scratch_bytes = (int64_t)(slots * slot_bytes);
+  GradTables gt;
+  GradScalars gs;
+  build_grad_tables(p->gap, p->ext, p->quality_offsets, &gt, &gs);
+  cudaStream_t st_ = e->stream;
+  auto put = [&](size_t o, const void* src, size_t n) -> int {
+    if (n) VD_CUDA(cudaMemcpyAsync(d + o, src, n, cudaMemcpyHostToDevice, st_));
+    return VD_OK;
+  };
+  if ((rc = put(o_rb, b->read_bases + b->read_off[0], read_bytes)) || (rc = put(o_rq, b->read_quals + b->read_off[0], read_bytes)) ||
+      (rc = put(o_roff, c.read_off.data(), c.read_off.size() * 8)) || (rc = put(o_rcode, c.read_code.data(), c.read_code.size() * 4)) ||
+      (rc = put(o_hb, b->hap_bases + b->hap_off[0], hap_bytes)) || (rc = put(o_hoff, c.hap_off.data(), c.hap_off.size() * 8)) ||
+      (rc = put(o_items, items.data(), items.size() * sizeof(RescueEntry))) || (rc = put(o_gt, &gt, sizeof(GradTables))))
+    return rc;
+  VD_CUDA(cudaMemsetAsync(d + o_cnt, 0, 64, st_));
+  BatchView bv{};
+  bv.read_bases = (const uint8_t*)(d + o_rb);
+  bv.read_quals = (const uint8_t*)(d + o_rq);
+  bv.read_off = (const int64_t*)(d + o_roff);
+  bv.read_code = (const int32_t*)(d + o_rcode);
+  bv.hap_bases = (const uint8_t*)(d + o_hb);
+  bv.hap_off = (const int64_t*)(d + o_hoff);
+  unsigned long long* cnt = (unsigned long long*)(d + o_cnt);
+  GradView gv{};
+  gv.out_ln = (double*)(d + o_ln);
+  gv.out_jac = (double*)(d + o_jac);
+  gv.scratch = d + o_scratch;
+  gv.slot_bytes = slot_bytes;
+  gv.store_all = store_all ? 1 : 0;
+  gv.error_flag = (int*)(cnt + 4);
+  const TableSet* dt = (const TableSet*)e->dtab.p;
+  const TableSet* ht = e->htab;
+  VD_CUDA(cudaEventRecord(e->ev_begin, st_));
+  cudaGetLastError();
+  if (!items.empty()) {
+    cudaError_t err;
+    if (!f64_only) {
+      gv.items = (const RescueEntry*)(d + o_items);
+      gv.count = nullptr;
+      gv.n_items = (long long)items.size();
+      gv.head = cnt + 0;
+      gv.spill = (RescueEntry*)(d + o_spill);
+      gv.spill_count = cnt + 2;
+      gv.spill_cap = (long long)items.size();
+      err = launch_grad_f32(bv, gv, &dt->f32, ht->s32, (const GradTables*)(d + o_gt), gs, grid32, st_);
+      if (err != cudaSuccess) return cuda_fail(err, "gradient FP32 pass launch");
+      ++s.kernel_launches;
+    }
+    gv.items = (const RescueEntry*)(d + (f64_only ? o_items : o_spill));
+    gv.count = f64_only ? nullptr : cnt + 2;
+    gv.n_items = (long long)items.size();
+    gv.head = cnt + 1;
+    gv.spill = nullptr;
+    gv.spill_count = nullptr;
+    gv.spill_cap = 0;
+    err = launch_grad_f64(bv, gv, &dt->f64, ht->s64, (const GradTables*)(d + o_gt), gs, grid64, st_);
+    if (err != cudaSuccess) return cuda_fail(err, "gradient FP64 pass launch");
+    ++s.kernel_launches;
+  }
+  VD_CUDA(cudaEventRecord(e->ev_end, st_));
+  // outputs: the kernels write every non-empty slot; empty pairs are -inf with a zero gradient
+  std::vector<double> ln((size_t)n_out), jac((size_t)n_out * 6);
+  unsigned long long hc[8];
+  if (n_out) {
+    VD_CUDA(cudaMemcpyAsync(ln.data(), d + o_ln, (size_t)n_out * 8, cudaMemcpyDeviceToHost, st_));
+    VD_CUDA(cudaMemcpyAsync(jac.data(), d + o_jac, (size_t)n_out * 48, cudaMemcpyDeviceToHost, st_));
+  }
+  VD_CUDA(cudaMemcpyAsync(hc, d + o_cnt, 64, cudaMemcpyDeviceToHost, st_));
+  VD_CUDA(cudaStreamSynchronize(st_));
+  float ms = 0.f;
+  VD_CUDA(cudaEventElapsedTime(&ms, e->ev_begin, e->ev_end));
+  s.kernel_ms = ms;
+  const unsigned flags = (unsigned)(hc[4] & 0xffffffffu);
+  if (flags & 1u) return fail(VD_EOVERFLOW, "gradient spill list overflow");
+  s.fp64_pairs = f64_only ? (int64_t)items.size() : (int64_t)hc[2];
+  for (int64_t o : empty_slots) {
+    ln[(size_t)o] = -HUGE_VAL;
+    for (int k = 0; k < 6; ++k) jac[(size_t)o * 6 + k] = 0.0;
+  }
+  for (int64_t k = 0; k < n_out; ++k) if (std::isnan(ln[(size_t)k])) ++s.failed_pairs;
+  std::memcpy(out_ln, ln.data(), (size_t)n_out * 8);
+  std::memcpy(out_jac, jac.data(), (size_t)n_out * 48);
+  s.total_ms = now_ms() - t0;
+  if (st) *st = s;
   return VD_OK;
 }
 

@@ -14,6 +14,19 @@ cudaError_t occupancy_f64(bool anchored, int* blocks_per_sm);
 cudaError_t launch_pair_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                             const Scalars<float>& sc, int grid, cudaStream_t stream);
 cudaError_t occupancy_pair_f32(int* blocks_per_sm);
+// gradient kernel (pairhmm_backward.cuh), FP32 and FP64 passes
+struct GradTables;
+struct GradScalars;
+struct GradView;
+cudaError_t launch_grad_f32(const BatchView& bv, const GradView& gv, const Tables<float>* tab,
+                            const Scalars<float>& sc, const GradTables* gt, const GradScalars& gs, int grid,
+                            cudaStream_t stream);
+cudaError_t launch_grad_f64(const BatchView& bv, const GradView& gv, const Tables<double>* tab,
+                            const Scalars<double>& sc, const GradTables* gt, const GradScalars& gs, int grid,
+                            cudaStream_t stream);
+cudaError_t occupancy_grad(bool fp64, int* blocks_per_sm);
+// bytes of one warp slot's checkpoints and segment buffer (sized for the FP64 pass)
+long long grad_slot_bytes(int R, int m, bool store_all);
 // sets the message vd_last_error returns on this thread; returns code
 int report_error(int code, const char* msg);
 // model tables for (gap, ext, optional per-bin Phred offsets), built on the host

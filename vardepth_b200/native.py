@@ -19,6 +19,7 @@ LIB_PATH = HERE / "libvardepth_pairhmm.so"
 VD_OK, VD_EINVAL, VD_ECUDA, VD_ENODEV, VD_ENOMEM, VD_EOVERFLOW = range(6)
 VD_PRECISION_MIXED, VD_PRECISION_FLOAT64 = 0, 1
 VD_SCHEDULE_BATCHED, VD_SCHEDULE_PLAIN = 0, 1
+VD_CHECKPOINT_SQRT, VD_CHECKPOINT_ALL = 0, 1
 
 c_i64 = ctypes.c_int64
 c_i32 = ctypes.c_int32
@@ -52,6 +53,15 @@ class VdStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class VdGradStats(ctypes.Structure):
+    _fields_ = [("pairs", c_i64), ("dp_cells", c_i64), ("fp64_pairs", c_i64), ("failed_pairs", c_i64),
+                ("scratch_bytes", c_i64), ("kernel_launches", c_i64), ("kernel_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # Every symbol include/vardepth_pairhmm.h declares, with its ctypes signature.
 SIGNATURES = {
     "vd_engine_create": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.POINTER(ctypes.c_void_p)]),
@@ -66,6 +76,8 @@ SIGNATURES = {
     "vd_plan_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdStats)]),
     "vd_plan_fetch": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
     "vd_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "vd_forward_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams),
+                                           ctypes.c_int, c_dp, c_dp, ctypes.POINTER(VdGradStats)]),
     "vd_pairhmm_pairs": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(c_u8p),
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_char_p),
                                         ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp]),
@@ -228,6 +240,17 @@ class Engine:
         check(library().vd_forward(self.handle, ctypes.byref(packed.batch), ctypes.byref(params),
                                    out.ctypes.data_as(c_dp), ctypes.byref(stats)), "vd_forward")
         return out, stats
+
+    def forward_backward(self, packed: Packed, params: VdParams, checkpoint: int = VD_CHECKPOINT_SQRT):
+        """ln L per output and d ln L / d(Qg, Qx, o0..o3) as an (outputs, 6) array."""
+        n = packed.n_outputs()
+        ln = np.empty(n, np.float64)
+        jac = np.empty((n, 6), np.float64)
+        stats = VdGradStats()
+        check(library().vd_forward_backward(self.handle, ctypes.byref(packed.batch), ctypes.byref(params),
+                                            int(checkpoint), ln.ctypes.data_as(c_dp), jac.ctypes.data_as(c_dp),
+                                            ctypes.byref(stats)), "vd_forward_backward")
+        return ln, jac, stats
 
     def plan(self, packed: Packed, params: VdParams) -> "Plan":
         return Plan(self, packed, params)

@@ -16,6 +16,14 @@ haplotypes are simulated (numpy.random.default_rng(seed), seeds 0-4):
 * ``config2``  2,000 regions x 4 haplotypes of U{1000..5000} bp; 50 reads of
   U{150..300} bp per region; 20% of the reads carry 5% substitution error with
   qualities U{2..15}.
+* ``config3``  1,000 regions shaped as config1, with reads drawn from the
+  PairHMM's own generative model under planted parameters: gap-open Q40,
+  gap-continuation Q8, and true base errors 10^(-(q + o_bin)/10) for the
+  reported quality q with bin offsets (+2, -1, 0, +3) (bins q<15, q<25,
+  q<35, q>=35, i.e. the Q10/20/30/40 levels).  A read starts in M at a
+  uniform column of its source haplotype; every M state moves to M, I or D
+  with 1-2g, g, g; I and D extend with x; M emits the haplotype base (a
+  uniform other base with probability e), I a uniform base, D nothing.
 * ``config4``  200,000 regions; haplotype length lognormal (median 400, sigma
   0.6) clipped to 80..8000, U{2..32} haplotypes; reads lognormal (median 40,
   sigma 1.0) clipped to 4..2000 of 150 bp; 2% of regions instead carry
@@ -257,8 +265,140 @@ def config2(seed: int = 2, n_regions: int = 2_000, gap: float = GAP_Q45, ext: fl
     return _assemble("config2", regions, gap, ext, {"seed": seed, "regions": n_regions})
 
 
-def config4(seed: int = 4, n_regions: int = 200_000, gap: float = GAP_Q45, ext: float = EXT_Q10) -> Workload:
+PLANTED_Q_GAP = 40.0
+PLANTED_Q_EXT = 8.0
+PLANTED_OFFSETS = (2.0, -1.0, 0.0, 3.0)
+
+
+def _quality_bin(q: np.ndarray) -> np.ndarray:
+    return np.searchsorted(np.array([15, 25, 35]), q, side="right")
+
+
+def _sim_hmm_reads(rng, haps, n_reads, lengths, gap, ext, offsets, quals_fn):
+    """Reads drawn from the PairHMM generative model (semiglobal, start uniform)."""
+    if n_reads == 0:
+        return [], []
+    src = rng.integers(0, len(haps), n_reads)
+    reads, quals = [], []
+    for k in range(n_reads):
+        hap = haps[src[k]]
+        m = len(hap)
+        n = int(min(lengths[k], m))
+        q = quals_fn(n)
+        ph = np.maximum(0.0, np.minimum(q, 60) + np.asarray(offsets)[_quality_bin(q)])
+        e = 10.0 ** (-ph / 10.0)
+        start = int(rng.integers(0, m - n + 1))
+        # one M -> {M, I, D} draw per emitted read base; gaps are rare, so the
+        # common all-match read is a straight copy
+        u = rng.random(n)
+        events = np.flatnonzero(u < 2 * gap)
+        if events.size == 0:
+            out = hap[start:start + n].copy()
+            from_hap = np.ones(n, bool)
+        else:
+            parts, flags = [], []
+            i = j = 0  # read bases emitted, haplotype column
+            j = start
+            ev = set(events.tolist())
+            while i < n:
+                if i in ev:
+                    run = 1 + int(rng.geometric(1.0 - ext)) - 1
+                    if u[i] < gap:       # insertion run: uniform bases
+                        take = min(run, n - i)
+                        parts.append(_random_hap(rng, take))
+                        flags.append(np.zeros(take, bool))
+                        i += take
+                        if i >= n:
+                            break
+                    else:                # deletion run: skip haplotype bases
+                        j += run
+                    ev.discard(i)
+                # M emission (past the haplotype end only insertions remain)
+                if j < m:
+                    parts.append(hap[j:j + 1])
+                    flags.append(np.ones(1, bool))
+                    j += 1
+                else:
+                    parts.append(_random_hap(rng, 1))
+                    flags.append(np.zeros(1, bool))
+                i += 1
+            out = np.concatenate(parts)[:n].copy()
+            from_hap = np.concatenate(flags)[:n]
+        sub = from_hap & (rng.random(n) < e)
+        if sub.any():
+            codes = np.searchsorted(ALPHABET, out[sub])
+            out[sub] = ALPHABET[(codes + rng.integers(1, 4, int(sub.sum()))) % 4]
+        reads.append(out)
+        quals.append(q)
+    return reads, quals
+
+
+def config3(seed: int = 3, n_regions: int = 1_000, q_gap: float = PLANTED_Q_GAP, q_ext: float = PLANTED_Q_EXT,
+            offsets=PLANTED_OFFSETS, sigma: float = 1.0) -> Workload:
+    """config1-shaped regions whose reads follow the model under planted parameters."""
     rng = np.random.default_rng(seed)
+    qf = _q_standard(rng)
+    gap, ext = 10.0 ** (-q_gap / 10.0), 10.0 ** (-q_ext / 10.0)
+    regions = []
+    for _ in range(n_regions):
+        H = int(rng.integers(2, 17))
+        hap0 = _random_hap(rng, int(rng.integers(100, 1001)))
+        haps = [hap0] + [_mutate(rng, hap0, int(rng.integers(1, 5)), int(rng.integers(1, 11))) for _ in range(H - 1)]
+        nr = int(np.clip(round(rng.lognormal(np.log(60), sigma)), 10, 500))
+        reads, quals = _sim_hmm_reads(rng, haps, nr, rng.integers(100, 251, nr), gap, ext, offsets, qf)
+        regions.append((haps, reads, quals))
+    return _assemble("config3", regions, GAP_Q45, EXT_Q10,
+                     {"seed": seed, "regions": n_regions, "planted": [q_gap, q_ext, *offsets]})
+
+
+def _concat(parts, name, gap, ext, meta) -> Workload:
+    """Join region batches generated separately into one batch."""
+    def join(key, off_key=None):
+        arrs = [getattr(p, key) for p in parts]
+        return np.concatenate(arrs) if arrs else np.empty(0)
+
+    def join_off(key):
+        out, base = [np.zeros(1, np.int64)], 0
+        for p in parts:
+            o = getattr(p, key)
+            out.append(o[1:] + base)
+            base += int(o[-1])
+        return np.concatenate(out)
+
+    return Workload(name, join("read_bases").astype(np.uint8), join("read_quals").astype(np.uint8),
+                    join_off("read_off"), join("hap_bases").astype(np.uint8), join_off("hap_off"),
+                    join_off("region_read_off"), join_off("region_hap_off"), gap, ext, False, meta)
+
+
+_CONFIG4_BLOCK = 2_000
+
+
+def _config4_block(args) -> Workload:
+    seed, block, count, gap, ext = args
+    rng = np.random.default_rng([seed, block])
+    return _config4_regions(rng, count, gap, ext)
+
+
+def config4(seed: int = 4, n_regions: int = 200_000, gap: float = GAP_Q45, ext: float = EXT_Q10,
+            workers: int = 0) -> Workload:
+    """Regions are drawn in blocks of 2,000, block b from default_rng([seed, b]), so the
+    blocks can be generated on several host processes (workers > 1; 0 = every core)."""
+    import os
+    blocks = [(seed, b, min(_CONFIG4_BLOCK, n_regions - b * _CONFIG4_BLOCK), gap, ext)
+              for b in range((n_regions + _CONFIG4_BLOCK - 1) // _CONFIG4_BLOCK)]
+    if workers == 0:
+        workers = min(len(blocks), len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else 1)
+    if workers > 1 and len(blocks) > 1:
+        import multiprocessing as mp
+        # spawn: a forked child of a process that holds a CUDA context can hang
+        with mp.get_context("spawn").Pool(workers) as pool:
+            parts = pool.map(_config4_block, blocks)
+    else:
+        parts = [_config4_block(b) for b in blocks]
+    return _concat(parts, "config4", gap, ext, {"seed": seed, "regions": n_regions})
+
+
+def _config4_regions(rng, n_regions: int, gap: float, ext: float) -> Workload:
     qf = _q_standard(rng)
     regions = []
     for _ in range(n_regions):
@@ -279,7 +419,7 @@ def config4(seed: int = 4, n_regions: int = 200_000, gap: float = GAP_Q45, ext: 
             nr = int(np.clip(round(rng.lognormal(np.log(40), 1.0)), 4, 2000))
             reads, quals = _sim_reads(rng, haps, nr, np.full(nr, 150), 0.01, 0.001, qf)
         regions.append((haps, reads, quals))
-    return _assemble("config4", regions, gap, ext, {"seed": seed, "regions": n_regions})
+    return _assemble("config4", regions, gap, ext, {})
 
 
 def random_pairs(seed: int, shapes, copies: int, qlo: int = 0, qhi: int = 61, alphabet="ACGT"):
