@@ -52,11 +52,40 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--regions", type=int, default=10_000)
+    ap.add_argument("--regions", type=int, default=0, help="regions of the workload (0: its full size)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
+                    help="run vardepth_b200.autotune on a 2%% region sample first (auto: configs[4] only)")
+    ap.add_argument("--workload", choices=["config1", "config2", "config3", "config4"], default="config1",
+                    help="config1 (default) is the metric's workload; the others print their own line")
     return ap.parse_args()
+
+
+WORKLOADS = {
+    "config1": "configs[1]: 10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of 100-250 bp, "
+               "gap-open Q45, gap-cont Q10",
+    "config2": "configs[2]: 2000 regions x 4 haps of 1000-5000 bp, 50 reads of 150-300 bp, 20% at 5% error "
+               "and Q2-Q15, gap-open Q45, gap-cont Q10",
+    "config3": "configs[3]: 1000 configs[1]-shaped regions simulated under gap-open Q40, gap-cont Q8, "
+               "bin offsets (+2,-1,0,+3); forward + reverse-wavefront gradient",
+    "config4": "configs[4]: 200000 regions, 2-32 haps of lognormal(400) 80-8000 bp, lognormal(40) reads of "
+               "150 bp, 2% of regions with 1-10 kb reads at 8% error, gap-open Q45, gap-cont Q10",
+}
+DEFAULT_REGIONS = {"config1": 10_000, "config2": 2_000, "config3": 1_000, "config4": 200_000}
+
+
+def make_workload(name, regions):
+    from vardepth_b200 import synthetic
+    if name == "config1":
+        return synthetic.config1(n_regions=regions)
+    if name == "config2":
+        return synthetic.config2(n_regions=regions)
+    if name == "config3":
+        return synthetic.config3(n_regions=regions)
+    return synthetic.config4(n_regions=regions, workers=0)
 
 
 # ---- CPU reference (oracle/_ref, the reference's own wide.cpp) -----------------------
@@ -202,8 +231,7 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from vardepth_b200 import synthetic
-    w = synthetic.config1(n_regions=args.regions)
+    w = make_workload(args.workload, args.regions)
     per_step = max(2.0, args.cpu_seconds)
     res = cpu_reference(w, per_step, repeats=0)
     jobs, cells, threads = res["jobs"], res["cells"], res["threads"]
@@ -216,8 +244,7 @@ def reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "configs[1]: 10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of "
-                                   "100-250 bp, gap-open Q45, gap-cont Q10", "regions": args.regions,
+            "config": {"workload": WORKLOADS[args.workload], "regions": args.regions,
                        "pairs": w.pairs(), "cells": w.cells(), "step": "one pass over the CPU sample"},
             "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
                              "sample": res["sample"]},
@@ -225,8 +252,81 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def gradient_arm(args, local):
+    """forward + reverse-wavefront gradient, checkpoint modes, accuracy and the fit."""
+    import torch
+    from vardepth_b200 import autograd as AG
+    from vardepth_b200 import native
+    w = make_workload("config3", args.regions)
+    packed = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
+                           region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
+    engine = native.Engine(local, 65536)
+    theta0 = np.array([45.0, 10.0, 0.0, 0.0, 0.0, 0.0])
+    params, _keep = AG.params_from_theta(theta0)
+    cells = w.cells()
+    modes = {}
+    launches = 0
+    for name, ck in (("sqrt", native.VD_CHECKPOINT_SQRT), ("all", native.VD_CHECKPOINT_ALL)):
+        for _ in range(max(1, args.warmup)):
+            engine.forward_backward(packed, params, ck)
+        torch.cuda.synchronize()
+        ms = wall = 0.0
+        for _ in range(args.steps):
+            ln, jac, st = engine.forward_backward(packed, params, ck)
+            ms += st.kernel_ms
+            wall += st.total_ms
+            launches += st.kernel_launches
+        modes[name] = {"gcups": round(cells / (ms / args.steps) / 1e6, 3), "kernel_ms": round(ms / args.steps, 3),
+                       "call_ms": round(wall / args.steps, 3), "scratch_bytes": int(st.scratch_bytes),
+                       "fp64_pairs": int(st.fp64_pairs), "failed_pairs": int(st.failed_pairs)}
+        if name == "sqrt":
+            ref_ln, ref_jac = ln, jac
+        elif not (np.array_equal(ln, ref_ln) and np.array_equal(jac, ref_jac)):
+            raise SystemExit("checkpoint modes disagree")
+    fw_ms = 0.0
+    for _ in range(args.steps):
+        _, fst = engine.forward(packed, params)
+        fw_ms += fst.kernel_ms
+    # gradient accuracy on a region subsample against the long-double expected-count oracle
+    from oracle import oracle as O
+    sub = np.random.default_rng(7).choice(w.n_regions, size=min(8, w.n_regions), replace=False)
+    offs = np.concatenate([[0], np.cumsum(np.diff(w.region_read_off) * np.diff(w.region_hap_off))])
+    idx = np.concatenate([np.arange(offs[g], offs[g + 1]) for g in sub])
+    sw = w.subset(sub)
+    pr, ph = sw.explicit_pairs()
+    lo, jo = O.grad_pairs(sw.read_bases, sw.read_quals, sw.read_off, sw.hap_bases, sw.hap_off, pr, ph,
+                          O.phred_to_prob(theta0[0]), O.phred_to_prob(theta0[1]), False, theta0[2:])
+    tot, want = ref_jac[idx].sum(0), jo.sum(0)
+    check = {"pairs": int(len(idx)), "oracle": "long-double expected-count gradient (oracle/)",
+             "summed_gradient_rel_err": [float(v) for v in np.abs(tot - want) / np.abs(want)],
+             "max_abs_dlog10": float(np.max(np.abs(ref_ln[idx] - lo)) / np.log(10.0))}
+    # the fit on every region, from Q45 / Q10 / zero offsets
+    batch = AG.Batch(engine, packed)
+    hist = []
+    t0 = time.perf_counter()
+    theta = AG.fit_error_model(batch, w.region_read_off, w.region_hap_off, theta0, history=hist)
+    fit_s = time.perf_counter() - t0
+    planted = np.array(w.meta["planted"])
+    line = {"metric": "PairHMM forward+gradient GCUPS on 1 B200 (configs[3])", "value": modes["sqrt"]["gcups"],
+            "unit": "GCUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": modes["sqrt"]["kernel_ms"], "higher_is_better": True, "dtype": "fp32",
+            "data": "synthetic", "config": {"workload": WORKLOADS["config3"], "regions": args.regions,
+                                            "pairs": w.pairs(), "cells": cells, "seed": w.meta.get("seed")},
+            "checkpointing": modes, "forward_gcups": round(cells / (fw_ms / args.steps) / 1e6, 3),
+            "gradient_check": check,
+            "fit": {"theta": [round(float(v), 4) for v in theta], "planted": planted.tolist(),
+                    "max_abs_err_phred": float(np.max(np.abs(theta.numpy() - planted))),
+                    "evaluations": len(hist), "seconds": round(fit_s, 2), "optimizer": "L-BFGS, FP32 theta",
+                    "objective": "sum over reads of ln mean_h L (region mixture)"},
+            "gpu_launches": launches}
+    print(json.dumps(line), flush=True)
+    engine.close()
+
+
 def main():
     args = parse()
+    if args.regions <= 0:
+        args.regions = DEFAULT_REGIONS[args.workload]
     if args.impl == "reference":
         reference_arm(args)
         return
@@ -242,8 +342,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
 
-    from vardepth_b200 import native, synthetic
-    w = synthetic.config1(n_regions=args.regions)
+    from vardepth_b200 import native
+    if args.workload == "config3":
+        gradient_arm(args, local)
+        return
+    w = make_workload(args.workload, args.regions)
     cells, pairs = w.cells(), w.pairs()
 
     def pinned(a):
@@ -278,6 +381,30 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # ---- autotuner: work-list choices timed on a region sample, kept on the engine ----
+    tuned = None
+    if args.autotune == "on" or (args.autotune == "auto" and args.workload == "config4"):
+        from vardepth_b200 import autotune
+        sub = w.subset(autotune.sample_regions(w.region_read_off, w.region_hap_off, fraction=0.02))
+        sp = native.Packed(sub.read_bases, sub.read_quals, sub.read_off, sub.hap_bases, sub.hap_off,
+                           region_read_off=sub.region_read_off, region_hap_off=sub.region_hap_off)
+        tlog = []
+        t0 = time.perf_counter()
+        best = autotune.autotune(engine, sp, params, use_cache=False, log=tlog)
+        tuned = {"chosen": {k: best[k] for k in autotune.DEFAULT}, "default": autotune.DEFAULT,
+                 "sample_regions": sub.n_regions, "sample_cells": sub.cells(),
+                 "sample_ms_default": best.get("default_ms"), "sample_ms_chosen": best.get("sample_ms"),
+                 "trials": tlog, "seconds": round(time.perf_counter() - t0, 2)}
+        if tuned["chosen"] != autotune.DEFAULT:
+            # the untuned schedule on the full batch, for the record
+            saved = engine.tuning()
+            engine.set_tuning(**autotune.DEFAULT)
+            uplan = engine.plan(packed, params)
+            uplan.run()
+            tuned["untuned_full_gcups"] = round(cells / uplan.run().kernel_ms / 1e6, 3)
+            uplan.close()
+            engine.set_tuning(**saved)
+
     # ---- device-resident batches (value) ----
     plan = engine.plan(packed, params)
     for _ in range(max(3, args.warmup)):
@@ -311,29 +438,36 @@ def main():
     plan.close()
 
     # ---- plain schedule on the same resident inputs (the batched-vs-plain comparison) ----
-    plain_params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED,
-                                         schedule=native.VD_SCHEDULE_PLAIN)
-    pplan = engine.plan(packed, plain_params)
-    for _ in range(args.warmup):
-        pplan.run()
-    barrier()
-    torch.cuda.synchronize()
-    plain_ms = plain_primary = 0.0
-    plain_steps = max(1, min(args.steps, 3))
-    plain_launches = 0
-    for _ in range(plain_steps):
-        st = pplan.run()
-        plain_ms += st.kernel_ms
-        plain_primary += st.primary_ms
-        plain_launches += st.kernel_launches
-    torch.cuda.synchronize()
-    barrier()
-    plain_ms = allmax(plain_ms) / plain_steps
-    plain_got = pplan.fetch()
-    pplan.close()
-    if not np.array_equal(plain_got, got):
-        raise SystemExit("plain and batched schedules disagree")
-    plain_value = world * cells / (plain_ms / 1e3) / 1e9
+    plain = None
+    if not args.no_plain:
+        plain_params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED,
+                                             schedule=native.VD_SCHEDULE_PLAIN)
+        pplan = engine.plan(packed, plain_params)
+        for _ in range(args.warmup):
+            pplan.run()
+        barrier()
+        torch.cuda.synchronize()
+        plain_ms = 0.0
+        plain_steps = max(1, min(args.steps, 3))
+        plain_launches = 0
+        for _ in range(plain_steps):
+            st = pplan.run()
+            plain_ms += st.kernel_ms
+            plain_launches += st.kernel_launches
+        torch.cuda.synchronize()
+        barrier()
+        plain_ms = allmax(plain_ms) / plain_steps
+        plain_got = pplan.fetch()
+        pplan.close()
+        if not np.array_equal(plain_got, got, equal_nan=True):
+            raise SystemExit("plain and batched schedules disagree")
+        plain_value = world * cells / (plain_ms / 1e3) / 1e9
+        plain = {"value": round(plain_value, 3), "unit": "GCUPS", "ms_per_step": round(plain_ms, 3),
+                 "steps": plain_steps, "gpu_launches": plain_launches,
+                 "batched_over_plain": round(value / plain_value, 3),
+                 "schedule": "VD_SCHEDULE_PLAIN: one pair per warp item, fixed 8 rows per lane, "
+                             "input order, static round-robin over a fixed grid; same tiers and "
+                             "arithmetic, results bit-identical to the batched schedule"}
 
     # ---- parity spot check on a region subsample (oracle, CPU) ----
     parity = None
@@ -393,10 +527,13 @@ def main():
                "kind": "reference", "sample": res["sample"]}
 
     primary_ms = allmax(primary_ms) / args.steps
-    achieved = cells * FLOPS_PER_CELL / (primary_ms / 1e3) / 1e12
+    # the primary tier holds all but ~0.5% of the work; elsewhere the
+    # FP64 tiers can hold a real share, so the whole step is the denominator
+    roof_ms = primary_ms if args.workload == "config1" else step_ms
+    achieved = cells * FLOPS_PER_CELL / (roof_ms / 1e3) / 1e12
     traffic = None
     tf = ROOT / "profiles" / "pairhmm_f32_traffic.json"
-    if tf.exists():
+    if tf.exists() and args.workload == "config1":
         try:
             t = json.loads(tf.read_text())
             traffic = t.get("bytes_per_launch_full_config1")
@@ -407,26 +544,23 @@ def main():
             "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": round(step_ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": "configs[1]: 10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of "
-                                   "100-250 bp, gap-open Q45, gap-cont Q10",
-                       "regions": args.regions, "pairs": pairs, "cells": cells, "seed": 1,
+            "config": {"workload": WORKLOADS[args.workload], "regions": args.regions, "pairs": pairs, "cells": cells,
+                       "seed": w.meta.get("seed"),
                        "inputs_bytes": w.input_bytes(), "l2": "inputs (%.2f GB) exceed the 126 MB L2; "
                        "the recurrence state lives in registers" % (w.input_bytes() / 1e9),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "precision": "FP32 scaled, FP64 rescue", "gpu": info["gpu"]},
             "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak.value, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / peak.value, 4), "traffic": traffic,
-                         "flops_per_cell": FLOPS_PER_CELL, "kernel": "pairhmm_kernel<float> (primary tier)",
+                         "flops_per_cell": FLOPS_PER_CELL,
+                         "kernel": "pairhmm_kernel<float> (primary tier)" if args.workload == "config1"
+                         else "all three tiers (whole step)",
                          "primary_ms": round(primary_ms, 3),
                          "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
                          "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},
-            "plain": {"value": round(plain_value, 3), "unit": "GCUPS", "ms_per_step": round(plain_ms, 3),
-                      "steps": plain_steps, "gpu_launches": plain_launches, "batched_over_plain": round(value / plain_value, 3),
-                      "schedule": "VD_SCHEDULE_PLAIN: one pair per warp item, fixed 8 rows per lane, "
-                                  "input order, static round-robin over a fixed grid; same tiers and "
-                                  "arithmetic, results bit-identical to the batched schedule"},
+            "plain": plain, "autotune": tuned,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "rescued_pairs": int(rescued), "parity": parity, "clocks": sampler.summary(),
+            "rescued_pairs": int(rescued), "rescued_fraction": round(rescued / max(1, pairs), 6), "parity": parity, "clocks": sampler.summary(),
         }
         print(json.dumps(line), flush=True)
     engine.close()

@@ -120,6 +120,21 @@ int vd_engine_destroy(vd_engine *engine);
 int vd_engine_info(const vd_engine *engine, char *name, int name_len, int *major, int *minor,
                    int *sm_count);
 
+/* Work-list choices of an engine, applied to the batches it builds from then
+ * on (the autotuner in vardepth_b200/autotune.py measures and sets them).
+ * No counterpart in the reference. */
+typedef struct vd_tuning {
+  int long_read_rows;   /* strip height of reads longer than 256 bases: 64, 128 or 256 (default);
+                           shorter strips are renormalised more often, so error-rich long reads
+                           stay in the FP32 tier */
+  int pair_mask;        /* bit R (1..8): two reads with R rows per lane may share a warp in the
+                           packed FP32 kernel (default 0x1fe: every R) */
+  int max_item_columns; /* haplotype columns one work item streams at most; 0 = unlimited (default) */
+  int reserved[5];      /* must be zero */
+} vd_tuning;
+int vd_engine_set_tuning(vd_engine *engine, const vd_tuning *tuning);
+int vd_engine_get_tuning(const vd_engine *engine, vd_tuning *tuning);
+
 /* Score a batch (host buffers in, host out).  Replaces CudaPairHMM.score
  * (accelerator.py:105-159): packing, transfers, the kernels and the FP64
  * rescue all happen here.  out must hold vd_batch_outputs(batch) doubles. */
@@ -197,6 +212,27 @@ typedef struct vd_grad_stats {
 
 int vd_forward_backward(vd_engine *engine, const vd_batch *batch, const vd_params *params, int checkpoint,
                         double *out_ln, double *out_jac, vd_grad_stats *stats);
+
+/* ---- region genotypes (forward + post-processing on the device) -----------
+ * Scores a region batch (region form) and, without copying the likelihoods
+ * back, normalises every read's row and sums each region's unordered diploid
+ * genotype log-likelihoods, all in FP64 on the device:
+ *   v_h = exp(ll_h - max ll), v'_h = (1 - e) v_h + e mean(v), e = 10^(-min(mq,60)/10),
+ *   certainty = max_h ln v'_h - min_h ln v'_h  (ln floored at 1e-300)
+ *     (caller/native/caller/molecule_rows.py:6-14 normalized_rows);
+ *   gl[(a,b)] for b = 0..H-1, a = 0..b (VCF order), over the region's reads:
+ *     artifact_prior < 0:  sum ln max(1e-300, (v'_a + v'_b)/2)
+ *       (caller/native/caller/triangular.py:13-16);
+ *     artifact_prior >= 0: the allele-balance (and, for a prior > 0,
+ *       contamination) mixture of caller/native/caller/mixture_general.cpp:9-37.
+ * Each read is one molecule (callers that merge mates pass merged rows to the
+ * reference's own mixture instead).  mapping_quality: one byte per read, NULL
+ * = 60.  out_gl holds sum_g H_g (H_g + 1) / 2 doubles (regions in order);
+ * out_ln, out_values (one per output of vd_forward) and out_certainty (one per
+ * read) may be NULL.  No counterpart in the reference as one call. */
+int vd_region_genotypes(vd_engine *engine, const vd_batch *batch, const vd_params *params,
+                        const unsigned char *mapping_quality, double artifact_prior, double *out_ln,
+                        double *out_values, double *out_certainty, double *out_gl, vd_stats *stats);
 
 /* ---- a call that allocates nothing ----------------------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc

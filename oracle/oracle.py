@@ -169,6 +169,48 @@ def fd_grad(read, qual, hap, theta, h=1e-3, anchored=False):
     return jac
 
 
+# ---- region post-processing (checker of vd_region_genotypes) ----------------------------
+
+def normalized_rows(ll, mapping_quality):
+    """caller/native/caller/molecule_rows.py:6-14: rows exp(ll - row max) mixed with the
+    mapping-quality error toward their mean; certainty = range of ln(max(1e-300, v))."""
+    ll = np.asarray(ll, np.float64)
+    err = 10.0 ** (-np.minimum(np.asarray(mapping_quality, np.int64), 60) / 10.0)
+    with np.errstate(invalid="ignore"):
+        v = np.exp(ll - ll.max(axis=1, keepdims=True))
+        v = (1 - err[:, None]) * v + err[:, None] * v.mean(axis=1, keepdims=True)
+        lv = np.log(np.maximum(1e-300, v))
+    return v, lv.max(axis=1) - lv.min(axis=1)
+
+
+_BALANCE = np.array([.2, .3, .4, .5, .6, .7, .8])
+_BALANCE_W = np.array([.025, .1, .225, .3, .225, .1, .025])
+_THETA = np.array([.02, .1, .2, .3])
+_THETA_W = np.array([.4, .35, .2, .05])
+
+
+def diploid_gl(v, artifact_prior=None):
+    """Unordered diploid genotype log-likelihoods in VCF order (b = 0..H-1, a = 0..b):
+    without a prior sum_rows ln max(1e-300, (v_a + v_b)/2) (triangular.py:13-16); with one the
+    allele-balance mixture over _BALANCE and, for a prior > 0, the contamination mixture over
+    _THETA x haplotypes, combined by log-sum-exp (mixture_general.cpp:9-37)."""
+    v = np.asarray(v, np.float64)
+    H = v.shape[1]
+    a, b = np.array([(a, b) for b in range(H) for a in range(b + 1)]).T
+    va, vb = v[:, a], v[:, b]
+    if artifact_prior is None:
+        return np.log(np.maximum(1e-300, (va + vb) / 2)).sum(axis=0)
+    clean = np.array([np.log(np.maximum(1e-300, w * va + (1 - w) * vb)).sum(axis=0) + np.log(q)
+                      for w, q in zip(_BALANCE, _BALANCE_W)])
+    clean = np.logaddexp.reduce(clean, axis=0)
+    if artifact_prior <= 0:
+        return clean
+    art = [np.log(np.maximum(1e-300, (1 - t) * (va + vb) / 2 + t * v[:, c, None])).sum(axis=0) + np.log(q / H)
+           for t, q in zip(_THETA, _THETA_W) for c in range(H)]
+    art = np.logaddexp.reduce(np.array(art), axis=0)
+    return np.logaddexp(np.log1p(-artifact_prior) + clean, np.log(artifact_prior) + art)
+
+
 def region_pairs(region_read_off, region_hap_off):
     """Explicit (read, hap) pairs of a region batch in the library's output order."""
     rr = np.asarray(region_read_off, np.int64)

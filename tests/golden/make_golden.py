@@ -17,6 +17,10 @@ used).  Shapes and seeds are those of the reference's tests:
                        wide.cpp read_haplotype_batch_mode
   config0_q30.npz      the same reads at the production 0.001 / 0.1 through
                        cpu_batch.pairs (trie_many, the production CPU path)
+  genotypes_seed4242.npz  12 configs[1]-shaped regions: ln L from wide.cpp
+                       read_haplotype_batch_mode, then per region molecule_rows.normalized_rows
+                       with seeded mapping qualities, triangular._diploid_likelihood_numpy (no
+                       prior) and mixture_cpu.general (mixture_general.cpp) at priors 0 and 0.001
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -190,6 +194,38 @@ def main():
     out["config0_q45"] = dict(base, semiglobal=q45.ravel(), gap=w.gap, ext=w.ext)
     prod = cpu_batch.many(seqs, qls, haps, mode=0)
     out["config0_q30"] = dict(base, semiglobal=np.asarray(prod).ravel(), gap=0.001, ext=0.1)
+
+    # region post-processing (molecule_rows.py, triangular.py, mixture_general.cpp)
+    blocks = types.ModuleType("blocks")
+    blocks.blocks_for = None
+    sys.modules["blocks"] = blocks
+    load_source("artifact", REFERENCE / "base" / "artifact.py")
+    rows = load_source("molecule_rows", REFERENCE / "molecule_rows.py")
+    tri = load_source("triangular", REFERENCE / "triangular.py")
+    mix = load_source("mixture_cpu", REFERENCE / "mixture_cpu.py")
+    w = synthetic.config1(seed=4242, n_regions=12)
+    mq = np.random.default_rng(4242).choice([0, 3, 20, 37, 60, 255], size=len(w.read_off) - 1).astype(np.uint8)
+    lns, vals, cert, gl_none, gl_p0, gl_p001 = [], [], [], [], [], []
+    for g in range(w.n_regions):
+        r0, r1 = w.region_read_off[g], w.region_read_off[g + 1]
+        h0, h1 = w.region_hap_off[g], w.region_hap_off[g + 1]
+        haps = [bytes(w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]]).decode() for h in range(h0, h1)]
+        ll = np.stack([O.ref_batch_mode(bytes(w.read_bases[w.read_off[r]:w.read_off[r + 1]]).decode(),
+                                        w.read_quals[w.read_off[r]:w.read_off[r + 1]], haps, gap=w.gap, ext=w.ext)
+                       for r in range(r0, r1)])
+        v, c = rows.normalized_rows(ll, mq[r0:r1])
+        lns.append(ll.ravel())
+        vals.append(v.ravel())
+        cert.append(c)
+        gl_none.append(tri._diploid_likelihood_numpy(v, None))
+        gl_p0.append(mix.general(v, 0.0, triangular=True))
+        gl_p001.append(mix.general(v, 0.001, triangular=True))
+    out["genotypes_seed4242"] = dict(
+        read_bases=w.read_bases, read_quals=w.read_quals, read_off=w.read_off, hap_bases=w.hap_bases,
+        hap_off=w.hap_off, region_read_off=w.region_read_off, region_hap_off=w.region_hap_off, mapping_quality=mq,
+        semiglobal=np.concatenate(lns), values=np.concatenate(vals), certainty=np.concatenate(cert),
+        gl_none=np.concatenate(gl_none), gl_prior0=np.concatenate(gl_p0), gl_prior001=np.concatenate(gl_p001),
+        gap=w.gap, ext=w.ext)
 
     for name, arrays in out.items():
         np.savez_compressed(HERE / f"{name}.npz", **{k: np.asarray(v) for k, v in arrays.items()})

@@ -321,3 +321,60 @@ def test_score_pairs_and_many_module_api(monkeypatch):
     assert_mixed_close(got.ravel(), want.ravel())
     flat = score_pairs([(r, q, h) for r, q in zip(reads, quals) for h in haps])
     np.testing.assert_array_equal(flat, got.ravel())
+
+
+@pytest.mark.parametrize("rows", [64, 128, 256])
+@pytest.mark.parametrize("anchored", [False, True])
+def test_long_read_strip_heights(rows, anchored):
+    """vd_tuning.long_read_rows: reads over 256 bases in strips of 64/128/256 rows, including
+    error-rich ones (8% substitutions at reported Q30) that underflow a 256-row FP32 strip."""
+    rng = np.random.default_rng(7 + rows)
+    pairs = []
+    for n, m, err in [(300, 420, 0.01), (700, 900, 0.08), (1500, 1700, 0.08), (2100, 2300, 0.03), (257, 400, 0.0)]:
+        hap = "".join(rng.choice(list("ACGT"), m))
+        start = int(rng.integers(0, m - n + 1))
+        read = list(hap[start:start + n])
+        for i in np.flatnonzero(rng.random(n) < err):
+            read[i] = "ACGT"[("ACGT".index(read[i]) + 1) % 4]
+        pairs.append(("".join(read), np.full(n, 30, np.uint8), hap))
+    want = np.array([O.forward(s, q, h, 0.001, 0.1, anchored) for s, q, h in pairs])
+    rb = np.frombuffer("".join(p[0] for p in pairs).encode(), np.uint8)
+    rq = np.concatenate([p[1] for p in pairs])
+    hb = np.frombuffer("".join(p[2] for p in pairs).encode(), np.uint8)
+    ro = np.concatenate([[0], np.cumsum([len(p[0]) for p in pairs])])
+    ho = np.concatenate([[0], np.cumsum([len(p[2]) for p in pairs])])
+    idx = np.arange(len(pairs), dtype=np.int32)
+    eng = native.Engine(0, 4096)
+    eng.set_tuning(long_read_rows=rows)
+    assert eng.tuning()["long_read_rows"] == rows
+    pk = native.Packed(rb, rq, ro, hb, ho, pair_read=idx, pair_hap=idx)
+    for precision in (native.VD_PRECISION_MIXED, native.VD_PRECISION_FLOAT64):
+        params, _ = native.make_params(0.001, 0.1, anchored, precision)
+        got, st = eng.forward(pk, params)
+        if precision == native.VD_PRECISION_FLOAT64:
+            np.testing.assert_allclose(got, want, rtol=0, atol=FP64_ATOL_LN * 10)
+        else:
+            assert_mixed_close(got, want)
+            if rows == 64 and not anchored:
+                # anchored pairs here force 120+ deletions (likelihoods far below the FP32
+                # range whatever the strip height) and are rescued in FP64 by design
+                assert st.rescued_fp64 + st.rescued_robust == 0
+    with pytest.raises(ValueError):
+        eng.set_tuning(long_read_rows=96)
+    eng.close()
+
+
+def test_autotune_on_a_sample():
+    from vardepth_b200 import autotune
+    w = S.config4(n_regions=120, workers=1)
+    sub = w.subset(autotune.sample_regions(w.region_read_off, w.region_hap_off, fraction=0.5, min_regions=40))
+    eng = native.Engine(0, 8192)
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    before, _ = eng.forward(_packed(w), params)
+    log = []
+    best = autotune.autotune(eng, _packed(sub), params, repeats=1, use_cache=False, log=log)
+    assert set(autotune.DEFAULT) <= set(best) and len(log) >= 3
+    assert eng.tuning() == {k: best[k] for k in autotune.DEFAULT}
+    after, _ = eng.forward(_packed(w), params)
+    assert_mixed_close(after, before)
+    eng.close()

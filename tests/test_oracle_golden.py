@@ -90,3 +90,22 @@ def test_reference_libraries_reproduce_golden():
     np.testing.assert_array_equal([O.ref_anchored(s, q, h) for s, q, h in pairs], d["anchored"])
     got = O.ref_pairhmm_pairs(pairs, mode=1)
     np.testing.assert_allclose(got, d["anchored"], atol=1e-9, rtol=0)
+
+
+def test_restatement_reproduces_region_postprocessing():
+    """normalized_rows (molecule_rows.py:6-14), _diploid_likelihood_numpy (triangular.py:13-16) and
+    mixture_general (mixture_general.cpp:9-37) as the reference computed them (genotypes_seed4242)."""
+    d = golden("genotypes_seed4242")
+    rro, rho = d["region_read_off"], d["region_hap_off"]
+    o = p0 = 0
+    for g in range(len(rro) - 1):
+        nr, H = int(rro[g + 1] - rro[g]), int(rho[g + 1] - rho[g])
+        v, c = O.normalized_rows(d["semiglobal"][o:o + nr * H].reshape(nr, H), d["mapping_quality"][rro[g]:rro[g + 1]])
+        np.testing.assert_array_equal(v.ravel(), d["values"][o:o + nr * H])
+        np.testing.assert_array_equal(c, d["certainty"][rro[g]:rro[g + 1]])
+        P = H * (H + 1) // 2
+        np.testing.assert_allclose(O.diploid_gl(v), d["gl_none"][p0:p0 + P], rtol=1e-13, atol=0)
+        np.testing.assert_allclose(O.diploid_gl(v, 0.0), d["gl_prior0"][p0:p0 + P], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(O.diploid_gl(v, 0.001), d["gl_prior001"][p0:p0 + P], rtol=1e-12, atol=0)
+        o += nr * H
+        p0 += P

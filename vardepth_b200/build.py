@@ -35,6 +35,7 @@ UNITS = [
     ("peak", "pairhmm_peak.cu", []),
     ("noalloc", "pairhmm_noalloc.cu", []),
     ("grad", "pairhmm_grad.cu", []),
+    ("genotype", "pairhmm_genotype.cu", []),
 ]
 
 

@@ -173,7 +173,9 @@ struct vd_engine {
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair = 0;                  // blocks of the two-read kernel
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
+  vd_tuning tuning{256, 0x1fe, 0, {0, 0, 0, 0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
+  DevBuf geno_arena;                  // buffers of vd_region_genotypes
   // table cache
   TableKey tkey{};
   bool tvalid = false;
@@ -282,9 +284,28 @@ int64_t batch_outputs(const vd_batch* b) {
   return total;
 }
 
-// Rows per lane for a read of n bases: the smallest R with 32 R >= n, at most
-// 8; longer reads are strip-mined in strips of 256 rows.
-int rows_per_lane(int n) { return std::min(kMaxR, std::max(1, (n + kWarp - 1) / kWarp)); }
+// Work-list choices the engine's tuning sets (vd_tuning).
+struct BuildOpts {
+  int long_R = kMaxR;              // rows per lane of reads longer than one 256-row strip
+  int pair_mask = 0x1fe;           // bit R: two reads of R rows per lane may share a warp
+  int64_t max_stream = 1 << 30;    // haplotype columns one work item streams at most
+};
+
+// Rows per lane for a read of n rows: the smallest R with 32 R >= n, at most
+// 8; longer reads are strip-mined in strips of 32 long_R rows.
+int rows_per_lane(int n, int long_R = kMaxR) {
+  if (n > kStripRows) return long_R;
+  return std::min(kMaxR, std::max(1, (n + kWarp - 1) / kWarp));
+}
+
+BuildOpts build_opts(const vd_engine* e) {
+  BuildOpts bo;
+  bo.long_R = e->tuning.long_read_rows / kWarp;
+  bo.pair_mask = e->tuning.pair_mask;
+  bo.max_stream = e->tuning.max_item_columns > 0 ? (int64_t)e->tuning.max_item_columns : (int64_t)1 << 30;
+  return bo;
+}
+
 
 // ---- host plan ------------------------------------------------------------------
 
@@ -366,7 +387,7 @@ struct ReadInfo {
   int32_t code;
 };
 
-ReadInfo read_info(const vd_batch* b, int64_t r, bool anchored) {
+ReadInfo read_info(const vd_batch* b, int64_t r, bool anchored, int long_R = kMaxR) {
   const int64_t o = b->read_off[r];
   const int n = (int)(b->read_off[r + 1] - o);
   ReadInfo ri{n, 0};
@@ -379,7 +400,7 @@ ReadInfo read_info(const vd_batch* b, int64_t r, bool anchored) {
   const bool gen = qmin < 2;
   // anchored reads carry one extra row on top: the emulator of row 0
   const int rows = n + (anchored ? 1 : 0);
-  ri.code = make_code(rows_per_lane(rows), gen, rows > kStripRows);
+  ri.code = make_code(rows_per_lane(rows, long_R), gen, rows > kStripRows);
   return ri;
 }
 
@@ -392,7 +413,8 @@ bool read_general(const vd_batch* b, int64_t r, const TableSet* ts) {
   return false;
 }
 
-void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bool offsets, bool anchored) {
+void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bool offsets, bool anchored,
+                         const BuildOpts& bo = BuildOpts()) {
   c.read_off.resize(c.rb - c.ra + 1);
   c.read_code.resize(c.rb - c.ra);
   const int64_t r0 = b->read_off[c.ra];
@@ -400,7 +422,7 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
     for (int64_t k = lo; k < hi; ++k) {
       const int64_t r = c.ra + k;
       c.read_off[k] = b->read_off[r] - r0;
-      ReadInfo ri = read_info(b, r, anchored);
+      ReadInfo ri = read_info(b, r, anchored, bo.long_R);
       if (offsets && ri.n > 0 && !code_general(ri.code) && read_general(b, r, ts))
         ri.code |= 256;
       c.read_code[k] = ri.code;
@@ -429,7 +451,8 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
 // fixed tile of kMaxR rows per lane, the list stays in input order and no
 // reads are paired.
 void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSet* ts, bool offsets,
-                        bool anchored, bool pair_reads, HostChunk& c, bool plain = false) {
+                        bool anchored, bool pair_reads, HostChunk& c, bool plain = false,
+                        const BuildOpts& bo = BuildOpts()) {
   if (plain) pair_reads = false;
   c.ra = b->region_read_off[g0];
   c.rb = b->region_read_off[g1];
@@ -438,8 +461,8 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   c.out_begin = 0;
   for (int64_t g = 0; g < g0; ++g)
     c.out_begin += (b->region_read_off[g + 1] - b->region_read_off[g]) * (b->region_hap_off[g + 1] - b->region_hap_off[g]);
-  finish_chunk_common(c, b, ts, offsets, anchored);
-  const int kMaxStream = 1 << 30;
+  finish_chunk_common(c, b, ts, offsets, anchored, bo);
+  const int64_t kMaxStream = bo.max_stream;
   // output offset of every region inside the chunk
   const int64_t ng = g1 - g0;
   std::vector<int64_t> region_out_of(ng + 1, 0);
@@ -508,7 +531,8 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       const int32_t code = c.read_code[r - c.ra];
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
       if (n <= 0) continue;
-      const bool eligible = pair_reads && !anchored && !code_general(code) && (code & 512) == 0;
+      const bool eligible = pair_reads && !anchored && !code_general(code) && (code & 512) == 0 &&
+                            ((bo.pair_mask >> code_R(code)) & 1);
       if (!eligible) { emit(r, -1); continue; }
       const int R = code_R(code);
       if (waiting[R] >= 0) {
@@ -559,14 +583,15 @@ void group_pairs(const vd_batch* b, PairGroups& pg) {
 }
 
 void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64_t rb, const TableSet* ts,
-                      bool offsets, bool anchored, HostChunk& c, bool plain = false) {
+                      bool offsets, bool anchored, HostChunk& c, bool plain = false,
+                      const BuildOpts& bo = BuildOpts()) {
   c.ra = ra;
   c.rb = rb;
   c.ha = 0;
   c.hb = b->n_haps;
-  finish_chunk_common(c, b, ts, offsets, anchored);
+  finish_chunk_common(c, b, ts, offsets, anchored, bo);
   std::vector<int64_t> cost;
-  const int kMaxStream = 1 << 30;
+  const int64_t kMaxStream = bo.max_stream;
   for (int64_t r = ra; r < rb; ++r) {
     const int32_t code = plain ? (c.read_code[r - ra] & ~15) | kMaxR : c.read_code[r - ra];
     const int n = (int)(c.read_off[r - ra + 1] - c.read_off[r - ra]);
@@ -1042,6 +1067,7 @@ int vd_engine_destroy(vd_engine* e) {
     }
     e->arena.release();
     e->grad_arena.release();
+    e->geno_arena.release();
     e->dtab.release();
     if (e->htab) cudaFreeHost(e->htab);
     if (e->ev_begin) cudaEventDestroy(e->ev_begin);
@@ -1060,6 +1086,24 @@ int vd_engine_info(const vd_engine* e, char* name, int name_len, int* major, int
   if (major) *major = e->cc_major;
   if (minor) *minor = e->cc_minor;
   if (sm_count) *sm_count = e->sm_count;
+  return VD_OK;
+}
+
+int vd_engine_set_tuning(vd_engine* e, const vd_tuning* t) {
+  if (!e || !t) return fail(VD_EINVAL, "engine or tuning is NULL");
+  if (t->long_read_rows != 64 && t->long_read_rows != 128 && t->long_read_rows != 256)
+    return fail(VD_EINVAL, "long_read_rows must be 64, 128 or 256");
+  if (t->pair_mask & ~0x1fe) return fail(VD_EINVAL, "pair_mask holds bits 1..8 only");
+  if (t->max_item_columns < 0) return fail(VD_EINVAL, "max_item_columns must be >= 0");
+  for (int i = 0; i < 5; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  std::lock_guard<std::mutex> lk(e->mu);
+  e->tuning = *t;
+  return VD_OK;
+}
+
+int vd_engine_get_tuning(const vd_engine* e, vd_tuning* t) {
+  if (!e || !t) return fail(VD_EINVAL, "engine or tuning is NULL");
+  *t = e->tuning;
   return VD_OK;
 }
 
@@ -1166,9 +1210,10 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     pl.ev_end = sl.ev[2];
     const double th = now_ms();
     const bool plain = p->schedule == VD_SCHEDULE_PLAIN;
-    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk, plain);
+    const BuildOpts bo = build_opts(e);
+    if (pair_form) build_pair_chunk(b, pg, u, u_end, e->htab, offsets, p->anchored != 0, pl.chunk, plain, bo);
     else build_region_chunk(b, u, u_end, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED,
-                            pl.chunk, plain);
+                            pl.chunk, plain, bo);
     HostChunk& c = pl.chunk;
     pl.L = layout_for(c, b, warps);
     s.host_ms += now_ms() - th;
@@ -1228,13 +1273,14 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
   }
   const bool offsets = p->quality_offsets != nullptr;
   const bool plain = p->schedule == VD_SCHEDULE_PLAIN;
+  const BuildOpts bo = build_opts(e);
   if (b->pair_read) {
     PairGroups pg;
     group_pairs(b, pg);
-    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, p->anchored != 0, pl->chunk, plain);
+    build_pair_chunk(b, pg, 0, b->n_reads, e->htab, offsets, p->anchored != 0, pl->chunk, plain, bo);
   } else {
     build_region_chunk(b, 0, b->n_regions, e->htab, offsets, p->anchored != 0, p->precision == VD_PRECISION_MIXED,
-                       pl->chunk, plain);
+                       pl->chunk, plain, bo);
   }
   pl->L = layout_for(pl->chunk, b, max_grid_warps(e));
   if ((rc = pl->own.reserve(pl->L.total))) { delete pl; return rc; }
@@ -1489,6 +1535,115 @@ int vd_forward_backward(vd_engine* e, const vd_batch* b, const vd_params* p, int
   for (int64_t k = 0; k < n_out; ++k) if (std::isnan(ln[(size_t)k])) ++s.failed_pairs;
   std::memcpy(out_ln, ln.data(), (size_t)n_out * 8);
   std::memcpy(out_jac, jac.data(), (size_t)n_out * 48);
+  s.total_ms = now_ms() - t0;
+  if (st) *st = s;
+  return VD_OK;
+}
+
+// ---- region post-processing ------------------------------------------------------------
+
+int vd_region_genotypes(vd_engine* e, const vd_batch* b, const vd_params* p, const unsigned char* mapping_quality,
+                        double artifact_prior, double* out_ln, double* out_values, double* out_certainty,
+                        double* out_gl, vd_stats* st) {
+  const double t0 = now_ms();
+  if (!e) return fail(VD_EINVAL, "engine is NULL");
+  int rc = validate_params(p);
+  if (!rc) rc = validate_batch(b);
+  if (rc) return rc;
+  if (b->pair_read) return fail(VD_EINVAL, "genotypes need the region form of the batch");
+  if (!(artifact_prior < 1.0) || std::isnan(artifact_prior)) return fail(VD_EINVAL, "artifact_prior must be < 1");
+  const int64_t G = b->n_regions;
+  // host layout: rows of the regions' reads, and per-region offsets
+  std::vector<int64_t> row_off, r_out(G), r_reads(G), gl_off(G + 1, 0), acc_off(G + 1, 0);
+  std::vector<int32_t> row_h, r_h(G);
+  std::vector<double> mq_err;
+  std::vector<int64_t> row_read;
+  int64_t out = 0;
+  for (int64_t g = 0; g < G; ++g) {
+    const int64_t r0 = b->region_read_off[g], r1 = b->region_read_off[g + 1];
+    const int64_t H = b->region_hap_off[g + 1] - b->region_hap_off[g];
+    if (H > 4096) return fail(VD_EINVAL, "genotypes support at most 4096 haplotypes per region");
+    r_out[g] = out;
+    r_reads[g] = r1 - r0;
+    r_h[g] = (int32_t)H;
+    const int64_t P = H * (H + 1) / 2;
+    const int64_t M = artifact_prior < 0.0 ? 1 : 7 + (artifact_prior > 0.0 ? 4 * H : 0);
+    gl_off[g + 1] = gl_off[g] + P;
+    acc_off[g + 1] = acc_off[g] + P * M;
+    for (int64_t r = r0; r < r1; ++r) {
+      row_off.push_back(out + (r - r0) * H);
+      row_h.push_back((int32_t)H);
+      row_read.push_back(r);
+      // caller/native/caller/molecule_rows.py:4 _MQ_ERROR
+      const unsigned q = mapping_quality ? mapping_quality[r] : 60u;
+      mq_err.push_back(std::pow(10.0, -(double)std::min(q, 60u) / 10.0));
+    }
+    out += (r1 - r0) * H;
+  }
+  const int64_t n_rows = (int64_t)row_off.size(), n_out = out;
+  if (n_out > 0 && !out_gl) return fail(VD_EINVAL, "out_gl is NULL");
+  vd_plan* pl = nullptr;
+  if ((rc = vd_plan_create(e, b, p, &pl))) return rc;
+  vd_stats s{};
+  if ((rc = vd_plan_run(pl, &s))) { vd_plan_destroy(pl); return rc; }
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard guard(e->device);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + std::max<size_t>(bytes, 1), 256); return o; };
+    const size_t o_roff = take(n_rows * 8), o_rh = take(n_rows * 4), o_mq = take(n_rows * 8),
+                 o_gout = take(G * 8), o_greads = take(G * 8), o_gh = take(G * 4), o_gloff = take((G + 1) * 8),
+                 o_accoff = take((G + 1) * 8), o_val = take(n_out * 8), o_cert = take(n_rows * 8),
+                 o_gl = take(gl_off[G] * 8), o_acc = take(acc_off[G] * 8);
+    rc = e->geno_arena.reserve(off);
+    char* d = (char*)e->geno_arena.p;
+    cudaStream_t sm = e->stream;
+    auto put = [&](size_t o, const void* src, size_t n) -> int {
+      if (n) VD_CUDA(cudaMemcpyAsync(d + o, src, n, cudaMemcpyHostToDevice, sm));
+      return VD_OK;
+    };
+    if (!rc && !(rc = put(o_roff, row_off.data(), n_rows * 8)) && !(rc = put(o_rh, row_h.data(), n_rows * 4)) &&
+        !(rc = put(o_mq, mq_err.data(), n_rows * 8)) && !(rc = put(o_gout, r_out.data(), G * 8)) &&
+        !(rc = put(o_greads, r_reads.data(), G * 8)) && !(rc = put(o_gh, r_h.data(), G * 4)) &&
+        !(rc = put(o_gloff, gl_off.data(), (G + 1) * 8)) && !(rc = put(o_accoff, acc_off.data(), (G + 1) * 8))) {
+      const double* dln = (const double*)(pl->base + pl->L.o_out);
+      cudaError_t err = cudaEventRecord(e->ev_begin, sm);
+      if (err == cudaSuccess)
+        err = launch_genotype_rows(dln, (const int64_t*)(d + o_roff), (const int32_t*)(d + o_rh),
+                                   (const double*)(d + o_mq), n_rows, (double*)(d + o_val), (double*)(d + o_cert),
+                                   e->sm_count, sm);
+      if (err == cudaSuccess)
+        err = launch_genotype_gl((const double*)(d + o_val), (const int64_t*)(d + o_gout),
+                                 (const int64_t*)(d + o_greads), (const int32_t*)(d + o_gh),
+                                 (const int64_t*)(d + o_gloff), (const int64_t*)(d + o_accoff), G, artifact_prior,
+                                 (double*)(d + o_acc), (double*)(d + o_gl), e->sm_count, sm);
+      if (err == cudaSuccess) err = cudaEventRecord(e->ev_end, sm);
+      std::vector<double> cert((size_t)n_rows);
+      if (err == cudaSuccess && gl_off[G])
+        err = cudaMemcpyAsync(out_gl, d + o_gl, gl_off[G] * 8, cudaMemcpyDeviceToHost, sm);
+      if (err == cudaSuccess && out_values && n_out)
+        err = cudaMemcpyAsync(out_values, d + o_val, n_out * 8, cudaMemcpyDeviceToHost, sm);
+      if (err == cudaSuccess && out_certainty && n_rows)
+        err = cudaMemcpyAsync(cert.data(), d + o_cert, n_rows * 8, cudaMemcpyDeviceToHost, sm);
+      if (err == cudaSuccess && out_ln && n_out)
+        err = cudaMemcpyAsync(out_ln, dln, n_out * 8, cudaMemcpyDeviceToHost, sm);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(sm);
+      float ms = 0.f;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e->ev_begin, e->ev_end);
+      if (err != cudaSuccess) {
+        rc = cuda_fail(err, "genotype post-processing");
+      } else {
+        if (out_certainty)
+          for (int64_t k = 0; k < n_rows; ++k) out_certainty[row_read[k]] = cert[(size_t)k];
+        s.kernel_ms += ms;
+        s.kernel_launches += 2;
+        s.d2h_bytes = gl_off[G] * 8 + (out_values ? n_out * 8 : 0) + (out_certainty ? n_rows * 8 : 0) +
+                      (out_ln ? n_out * 8 : 0);
+      }
+    }
+  }
+  vd_plan_destroy(pl);
+  if (rc) return rc;
   s.total_ms = now_ms() - t0;
   if (st) *st = s;
   return VD_OK;

@@ -231,6 +231,33 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       }
     };
 
+    // Boundary records of the strip above, for lane 0 (whose stream position is
+    // the step index t): each lane loads one record of the next 32 positions in
+    // one coalesced access, a window ahead of use, and a shuffle hands lane 0
+    // its record, so no step waits on memory.  A position is read here before
+    // lane 31 overwrites it with this strip's own boundary (31 or more steps
+    // later, past a __syncwarp).
+    T2 pf_cur = {T(0), T(0)}, pf_nxt = {T(0), T(0)};
+    auto pf_load = [&](int base) -> T2 {
+      const long long q = (long long)base + lane;
+      return q < qv.scratch_stride ? scratch[q] : T2{T(0), T(0)};
+    };
+    if (!FIRST) {
+      pf_cur = pf_load(0);
+      pf_nxt = pf_load(kWarp);
+    }
+    auto boundary = [&](int t) -> T2 {
+      const int k = t & (kWarp - 1);
+      if (k == 0 && t > 0) {
+        pf_cur = pf_nxt;
+        pf_nxt = pf_load(t + kWarp);
+      }
+      T2 r;
+      r.x = __shfl_sync(FULL, pf_cur.x, k);
+      r.y = __shfl_sync(FULL, pf_cur.y, k);
+      return r;
+    };
+
     // step with per-lane haplotype bookkeeping (ramps and short haplotypes)
     auto gstep = [&](int t) {
       const int p = t - lane;
@@ -259,8 +286,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         iu = ANCH ? T(0) : c0;
         is = iu;
       } else {
-        T2 rec = {T(0), T(0)};
-        if (lane == 0 && active) rec = scratch[p];
+        T2 rec = boundary(t);
+        if (!active) rec = T2{T(0), T(0)};
         iu = rec.y;
         is = rec.x;
       }
@@ -282,7 +309,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     };
 
     // step with every lane inside the same haplotype at a column >= 1
-    auto sstep = [&](uint32_t hb, int p) {
+    auto sstep = [&](uint32_t hb, int p, int t) {
       T u_in = __shfl_up_sync(FULL, u_bot, 1);
       T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
       T iu, is;
@@ -290,8 +317,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         iu = ANCH ? T(0) : c0;
         is = iu;
       } else {
-        T2 rec = {T(0), T(0)};
-        if (lane == 0) rec = scratch[p];
+        const T2 rec = boundary(t);
         iu = rec.y;
         is = rec.x;
       }
@@ -324,12 +350,12 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         for (; t + kUnroll <= Snext; t += kUnroll) {
           const uint8_t* q = hp + (t - lane);
 #pragma unroll
-          for (int u = 0; u < kUnroll; ++u) sstep((uint32_t)q[u], t - lane + u);
+          for (int u = 0; u < kUnroll; ++u) sstep((uint32_t)q[u], t - lane + u, t + u);
           if (last && !ANCH) { acc64 += (double)acc32; acc32 = T(0); }
           if (!last) __syncwarp();
         }
         for (; t < Snext; ++t) {
-          sstep((uint32_t)hp[t - lane], t - lane);
+          sstep((uint32_t)hp[t - lane], t - lane, t);
           if (last && !ANCH) { acc64 += (double)acc32; acc32 = T(0); }
         }
       }
@@ -360,13 +386,13 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
 
   if (nstrips == 1) {
     run_strip(std::true_type{}, std::true_type{}, 0);
-  } else if constexpr (R == kMaxR || R == 1) {
+  } else if constexpr (R == kMaxR || R == 4 || R == 2 || R == 1) {
     bool ok = run_strip(std::true_type{}, std::false_type{}, 0);
     for (int strip = 1; ok && strip < nstrips - 1; ++strip) ok = run_strip(std::false_type{}, std::false_type{}, strip);
     if (ok) ok = run_strip(std::false_type{}, std::true_type{}, nstrips - 1);
     fail = !ok;
   } else {
-    fail = true;  // not reached: reads longer than one strip run with R = 8 (R = 1 in the robust tier)
+    fail = true;  // not reached: reads longer than one strip run with R = 8, 4 or 2 (1 in the robust tier)
   }
 
   if (fail) {

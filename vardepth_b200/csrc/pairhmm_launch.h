@@ -27,6 +27,14 @@ cudaError_t launch_grad_f64(const BatchView& bv, const GradView& gv, const Table
 cudaError_t occupancy_grad(bool fp64, int* blocks_per_sm);
 // bytes of one warp slot's checkpoints and segment buffer (sized for the FP64 pass)
 long long grad_slot_bytes(int R, int m, bool store_all);
+// region post-processing (pairhmm_genotype.cu)
+cudaError_t launch_genotype_rows(const double* ln, const int64_t* row_off, const int32_t* row_h,
+                                 const double* mq_error, int64_t n_reads, double* values, double* certainty,
+                                 int sm_count, cudaStream_t stream);
+cudaError_t launch_genotype_gl(const double* values, const int64_t* region_out_off, const int64_t* region_reads,
+                               const int32_t* region_h, const int64_t* gl_off, const int64_t* acc_off,
+                               int64_t n_regions, double prior, double* acc, double* gl, int sm_count,
+                               cudaStream_t stream);
 // sets the message vd_last_error returns on this thread; returns code
 int report_error(int code, const char* msg);
 // model tables for (gap, ext, optional per-bin Phred offsets), built on the host

@@ -53,6 +53,15 @@ class VdStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class VdTuning(ctypes.Structure):
+    _fields_ = [("long_read_rows", ctypes.c_int), ("pair_mask", ctypes.c_int), ("max_item_columns", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
+
+    def as_dict(self) -> dict:
+        return {"long_read_rows": self.long_read_rows, "pair_mask": self.pair_mask,
+                "max_item_columns": self.max_item_columns}
+
+
 class VdGradStats(ctypes.Structure):
     _fields_ = [("pairs", c_i64), ("dp_cells", c_i64), ("fp64_pairs", c_i64), ("failed_pairs", c_i64),
                 ("scratch_bytes", c_i64), ("kernel_launches", c_i64), ("kernel_ms", ctypes.c_double),
@@ -68,6 +77,11 @@ SIGNATURES = {
     "vd_engine_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "vd_engine_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "vd_region_genotypes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams),
+                                           c_u8p, ctypes.c_double, c_dp, c_dp, c_dp, c_dp,
+                                           ctypes.POINTER(VdStats)]),
+    "vd_engine_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdTuning)]),
+    "vd_engine_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdTuning)]),
     "vd_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams), c_dp,
                                   ctypes.POINTER(VdStats)]),
     "vd_batch_outputs": (c_i64, [ctypes.POINTER(VdBatch)]),
@@ -232,6 +246,16 @@ class Engine:
                                        ctypes.byref(sms)), "vd_engine_info")
         return {"gpu": name.value.decode(), "compute_capability": [major.value, minor.value], "sm_count": sms.value}
 
+    def tuning(self) -> dict:
+        t = VdTuning()
+        check(library().vd_engine_get_tuning(self.handle, ctypes.byref(t)), "vd_engine_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, long_read_rows: int = 256, pair_mask: int = 0x1FE, max_item_columns: int = 0) -> None:
+        t = VdTuning()
+        t.long_read_rows, t.pair_mask, t.max_item_columns = int(long_read_rows), int(pair_mask), int(max_item_columns)
+        check(library().vd_engine_set_tuning(self.handle, ctypes.byref(t)), "vd_engine_set_tuning")
+
     def forward(self, packed: Packed, params: VdParams, out: np.ndarray | None = None):
         n = packed.n_outputs()
         if out is None:
@@ -251,6 +275,34 @@ class Engine:
                                             int(checkpoint), ln.ctypes.data_as(c_dp), jac.ctypes.data_as(c_dp),
                                             ctypes.byref(stats)), "vd_forward_backward")
         return ln, jac, stats
+
+    def region_genotypes(self, packed: Packed, params: VdParams, mapping_quality=None, artifact_prior=None,
+                         values: bool = True, certainty: bool = True, ln: bool = True) -> dict:
+        """Forward pass plus on-device normalised rows and diploid genotype log-likelihoods of
+        every region (vd_region_genotypes); ``gl`` is a list with one array per region."""
+        if packed.pair_read is not None:
+            raise ValueError("genotypes need the region form of the batch")
+        rr = np.diff(packed.region_read_off)
+        hh = np.diff(packed.region_hap_off)
+        n_out = int(np.sum(rr * hh))
+        P = hh * (hh + 1) // 2
+        gl = np.empty(int(P.sum()), np.float64)
+        out = {"ln": np.empty(n_out) if ln else None, "values": np.empty(n_out) if values else None,
+               "certainty": np.full(len(packed.read_off) - 1, np.nan) if certainty else None}
+        mq = None if mapping_quality is None else np.ascontiguousarray(mapping_quality, np.uint8)
+        if mq is not None and len(mq) != len(packed.read_off) - 1:
+            raise ValueError("one mapping quality per read")
+        prior = -1.0 if artifact_prior is None else float(artifact_prior)
+        stats = VdStats()
+        opt = lambda a: a.ctypes.data_as(c_dp) if a is not None else ctypes.cast(None, c_dp)
+        check(library().vd_region_genotypes(self.handle, ctypes.byref(packed.batch), ctypes.byref(params),
+                                            _ptr(mq, ctypes.c_ubyte), prior, opt(out["ln"]), opt(out["values"]),
+                                            opt(out["certainty"]), gl.ctypes.data_as(c_dp), ctypes.byref(stats)),
+              "vd_region_genotypes")
+        offs = np.concatenate([[0], np.cumsum(P)])
+        out["gl"] = [gl[offs[g]:offs[g + 1]] for g in range(len(P))]
+        out["stats"] = stats
+        return out
 
     def plan(self, packed: Packed, params: VdParams) -> "Plan":
         return Plan(self, packed, params)

@@ -380,9 +380,11 @@ def _config4_block(args) -> Workload:
 
 
 def config4(seed: int = 4, n_regions: int = 200_000, gap: float = GAP_Q45, ext: float = EXT_Q10,
-            workers: int = 0) -> Workload:
+            workers: int = 1) -> Workload:
     """Regions are drawn in blocks of 2,000, block b from default_rng([seed, b]), so the
-    blocks can be generated on several host processes (workers > 1; 0 = every core)."""
+    blocks can be generated on several host processes (workers > 1; 0 = every core).  The
+    processes are spawned, so a script that asks for workers != 1 must call this under
+    ``if __name__ == "__main__":``."""
     import os
     blocks = [(seed, b, min(_CONFIG4_BLOCK, n_regions - b * _CONFIG4_BLOCK), gap, ext)
               for b in range((n_regions + _CONFIG4_BLOCK - 1) // _CONFIG4_BLOCK)]
