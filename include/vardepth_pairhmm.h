@@ -228,11 +228,27 @@ int vd_forward_backward(vd_engine *engine, const vd_batch *batch, const vd_param
  * Each read is one molecule (callers that merge mates pass merged rows to the
  * reference's own mixture instead).  mapping_quality: one byte per read, NULL
  * = 60.  out_gl holds sum_g H_g (H_g + 1) / 2 doubles (regions in order);
- * out_ln, out_values (one per output of vd_forward) and out_certainty (one per
- * read) may be NULL.  No counterpart in the reference as one call. */
+ * out_ln, out_values (one per output of vd_forward), out_certainty (one per
+ * read) and out_guarded (one int per region) may be NULL.
+ *
+ * Near-tie guard (options->near_tie_guard = 1; the device-side counterpart of
+ * caller/native/caller/partial_anchor.py:120-133): a region whose best two
+ * genotypes lie within 1e-4 x max(1, reads) of each other, by GL or by GL
+ * plus the uniform haplotype prior (1 for a == b, 2 otherwise), is flagged on
+ * the device and rescored in FP64 (VD_PRECISION_FLOAT64, within 2e-9 of the
+ * reference's CPU FP64), so its genotype call follows the FP64 convention;
+ * out_guarded[g] = 1 marks those regions.  No counterpart in the reference as
+ * one call. */
+typedef struct vd_genotype_options {
+  double artifact_prior;  /* < 0: no artifact prior; >= 0: the mixtures above */
+  int near_tie_guard;     /* 1: rescore near-tied regions in FP64 */
+  int reserved[3];        /* must be zero */
+} vd_genotype_options;
+
 int vd_region_genotypes(vd_engine *engine, const vd_batch *batch, const vd_params *params,
-                        const unsigned char *mapping_quality, double artifact_prior, double *out_ln,
-                        double *out_values, double *out_certainty, double *out_gl, vd_stats *stats);
+                        const unsigned char *mapping_quality, const vd_genotype_options *options,
+                        double *out_ln, double *out_values, double *out_certainty, double *out_gl,
+                        int *out_guarded, vd_stats *stats);
 
 /* ---- a call that allocates nothing ----------------------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc

@@ -82,3 +82,30 @@ def test_mixed_precision_calls_and_optional_outputs(engine):
         pr, ph = w.explicit_pairs()
         engine.region_genotypes(native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
                                               pair_read=pr, pair_hap=ph), params)
+
+
+def test_near_tie_guard_rescores_tied_regions_in_fp64(engine):
+    """partial_anchor.py:120-133 as a device flag: a region whose haplotypes are identical ties every
+    genotype and is rescored in FP64; a region with a clear call keeps its mixed-precision result."""
+    w = S.config1(n_regions=6, seed=21)
+    # region 0 gets two copies of its first haplotype
+    haps = [w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]] for h in range(len(w.hap_off) - 1)]
+    h0 = w.region_hap_off[0]
+    haps[h0 + 1] = haps[h0].copy()
+    hap_bases = np.concatenate(haps)
+    hap_off = np.concatenate([[0], np.cumsum([len(h) for h in haps])])
+    pk = native.Packed(w.read_bases, w.read_quals, w.read_off, hap_bases, hap_off,
+                       region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
+    mq = np.full(len(w.read_off) - 1, 60, np.uint8)
+    mixed, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    fp64, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_FLOAT64)
+    plain = engine.region_genotypes(pk, mixed, mq, 0.001)
+    guarded = engine.region_genotypes(pk, mixed, mq, 0.001, near_tie_guard=True)
+    exact = engine.region_genotypes(pk, fp64, mq, 0.001)
+    assert guarded["guarded"][0] and guarded["stats"].rescued_fp64 > 0
+    for g in range(w.n_regions):
+        want = exact if guarded["guarded"][g] else plain
+        np.testing.assert_array_equal(guarded["gl"][g], want["gl"][g])
+    nr, H = int(w.region_read_off[1]), int(w.region_hap_off[1])
+    np.testing.assert_array_equal(guarded["ln"][:nr * H], exact["ln"][:nr * H])
+    np.testing.assert_array_equal(guarded["certainty"][:nr], exact["certainty"][:nr])

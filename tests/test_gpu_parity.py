@@ -378,3 +378,19 @@ def test_autotune_on_a_sample():
     after, _ = eng.forward(_packed(w), params)
     assert_mixed_close(after, before)
     eng.close()
+
+
+def test_region_shards_score_like_the_whole_batch():
+    """Each rank's shard (LPT by cells) scored on its own gives the whole batch's values."""
+    from vardepth_b200 import shard
+    w = S.config1(n_regions=50, seed=9)
+    pk = _packed(w)
+    eng = native.Engine(0, 4096)
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    whole, _ = eng.forward(pk, params)
+    full = np.full(pk.n_outputs(), np.nan)
+    for part in shard.shard_regions(shard.region_cells(pk), 3):
+        sub, pos = shard.subset(pk, part)
+        full[pos] = eng.forward(sub, params)[0]
+    np.testing.assert_array_equal(full, whole)
+    eng.close()

@@ -140,7 +140,43 @@ __global__ void gl_kernel(const double* __restrict__ values, const int64_t* __re
   }
 }
 
+// One thread per region: flags the regions whose best two genotypes lie within
+// 1e-4 x max(1, reads) of each other, by GL or by GL plus the uniform
+// haplotype prior (1 for a == b, 2 otherwise, normalised), as the numerical
+// guard of caller/native/caller/partial_anchor.py:120-133 measures it.
+__global__ void tie_kernel(const double* __restrict__ gl, const int64_t* __restrict__ gl_off,
+                           const int32_t* __restrict__ region_h, const int64_t* __restrict__ region_reads,
+                           int64_t n_regions, int* __restrict__ flags) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_regions;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int H = region_h[g];
+    const int P = H * (H + 1) / 2;
+    if (P < 2) { flags[g] = 0; continue; }
+    const double* v = gl + gl_off[g];
+    const double lnH2 = 2.0 * log((double)H);
+    double a1 = -HUGE_VAL, a2 = -HUGE_VAL, b1 = -HUGE_VAL, b2 = -HUGE_VAL;
+    int p = 0;
+    for (int b = 0; b < H; ++b)
+      for (int a = 0; a <= b; ++a, ++p) {
+        const double x = v[p];
+        const double y = x + (a == b ? 0.0 : 0.6931471805599453094) - lnH2;
+        if (x > a1) { a2 = a1; a1 = x; } else if (x > a2) { a2 = x; }
+        if (y > b1) { b2 = b1; b1 = y; } else if (y > b2) { b2 = y; }
+      }
+    const double margin = 1e-4 * fmax(1.0, (double)region_reads[g]);
+    flags[g] = fmin(a1 - a2, b1 - b2) <= margin ? 1 : 0;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_genotype_ties(const double* gl, const int64_t* gl_off, const int32_t* region_h,
+                                 const int64_t* region_reads, int64_t n_regions, int* flags, cudaStream_t stream) {
+  if (n_regions <= 0) return cudaSuccess;
+  const int grid = (int)((n_regions + 255) / 256 < 1024 ? (n_regions + 255) / 256 : 1024);
+  tie_kernel<<<grid, 256, 0, stream>>>(gl, gl_off, region_h, region_reads, n_regions, flags);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_genotype_rows(const double* ln, const int64_t* row_off, const int32_t* row_h,
                                  const double* mq_error, int64_t n_reads, double* values, double* certainty,

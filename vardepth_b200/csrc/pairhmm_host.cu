@@ -1543,15 +1543,19 @@ int vd_forward_backward(vd_engine* e, const vd_batch* b, const vd_params* p, int
 // ---- region post-processing ------------------------------------------------------------
 
 int vd_region_genotypes(vd_engine* e, const vd_batch* b, const vd_params* p, const unsigned char* mapping_quality,
-                        double artifact_prior, double* out_ln, double* out_values, double* out_certainty,
-                        double* out_gl, vd_stats* st) {
+                        const vd_genotype_options* opt, double* out_ln, double* out_values, double* out_certainty,
+                        double* out_gl, int* out_guarded, vd_stats* st) {
   const double t0 = now_ms();
   if (!e) return fail(VD_EINVAL, "engine is NULL");
   int rc = validate_params(p);
   if (!rc) rc = validate_batch(b);
   if (rc) return rc;
   if (b->pair_read) return fail(VD_EINVAL, "genotypes need the region form of the batch");
+  if (!opt) return fail(VD_EINVAL, "options is NULL");
+  const double artifact_prior = opt->artifact_prior;
   if (!(artifact_prior < 1.0) || std::isnan(artifact_prior)) return fail(VD_EINVAL, "artifact_prior must be < 1");
+  if (opt->near_tie_guard != 0 && opt->near_tie_guard != 1) return fail(VD_EINVAL, "near_tie_guard must be 0 or 1");
+  for (int i = 0; i < 3; ++i) if (opt->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
   const int64_t G = b->n_regions;
   // host layout: rows of the regions' reads, and per-region offsets
   std::vector<int64_t> row_off, r_out(G), r_reads(G), gl_off(G + 1, 0), acc_off(G + 1, 0);
@@ -1581,20 +1585,22 @@ int vd_region_genotypes(vd_engine* e, const vd_batch* b, const vd_params* p, con
     out += (r1 - r0) * H;
   }
   const int64_t n_rows = (int64_t)row_off.size(), n_out = out;
-  if (n_out > 0 && !out_gl) return fail(VD_EINVAL, "out_gl is NULL");
+  if (gl_off[G] > 0 && !out_gl) return fail(VD_EINVAL, "out_gl is NULL");
+  const bool guard = opt->near_tie_guard == 1 && p->precision != VD_PRECISION_FLOAT64;
+  std::vector<int> flags((size_t)G, 0);
   vd_plan* pl = nullptr;
   if ((rc = vd_plan_create(e, b, p, &pl))) return rc;
   vd_stats s{};
   if ((rc = vd_plan_run(pl, &s))) { vd_plan_destroy(pl); return rc; }
   {
     std::lock_guard<std::mutex> lk(e->mu);
-    DeviceGuard guard(e->device);
+    DeviceGuard dguard(e->device);
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + std::max<size_t>(bytes, 1), 256); return o; };
     const size_t o_roff = take(n_rows * 8), o_rh = take(n_rows * 4), o_mq = take(n_rows * 8),
                  o_gout = take(G * 8), o_greads = take(G * 8), o_gh = take(G * 4), o_gloff = take((G + 1) * 8),
                  o_accoff = take((G + 1) * 8), o_val = take(n_out * 8), o_cert = take(n_rows * 8),
-                 o_gl = take(gl_off[G] * 8), o_acc = take(acc_off[G] * 8);
+                 o_gl = take(gl_off[G] * 8), o_acc = take(acc_off[G] * 8), o_flag = take(G * 4);
     rc = e->geno_arena.reserve(off);
     char* d = (char*)e->geno_arena.p;
     cudaStream_t sm = e->stream;
@@ -1617,6 +1623,10 @@ int vd_region_genotypes(vd_engine* e, const vd_batch* b, const vd_params* p, con
                                  (const int64_t*)(d + o_greads), (const int32_t*)(d + o_gh),
                                  (const int64_t*)(d + o_gloff), (const int64_t*)(d + o_accoff), G, artifact_prior,
                                  (double*)(d + o_acc), (double*)(d + o_gl), e->sm_count, sm);
+      if (err == cudaSuccess && guard)
+        err = launch_genotype_ties((const double*)(d + o_gl), (const int64_t*)(d + o_gloff),
+                                   (const int32_t*)(d + o_gh), (const int64_t*)(d + o_greads), G, (int*)(d + o_flag),
+                                   sm);
       if (err == cudaSuccess) err = cudaEventRecord(e->ev_end, sm);
       std::vector<double> cert((size_t)n_rows);
       if (err == cudaSuccess && gl_off[G])
@@ -1627,6 +1637,8 @@ int vd_region_genotypes(vd_engine* e, const vd_batch* b, const vd_params* p, con
         err = cudaMemcpyAsync(cert.data(), d + o_cert, n_rows * 8, cudaMemcpyDeviceToHost, sm);
       if (err == cudaSuccess && out_ln && n_out)
         err = cudaMemcpyAsync(out_ln, dln, n_out * 8, cudaMemcpyDeviceToHost, sm);
+      if (err == cudaSuccess && guard && G)
+        err = cudaMemcpyAsync(flags.data(), d + o_flag, G * 4, cudaMemcpyDeviceToHost, sm);
       if (err == cudaSuccess) err = cudaStreamSynchronize(sm);
       float ms = 0.f;
       if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e->ev_begin, e->ev_end);
@@ -1636,14 +1648,84 @@ int vd_region_genotypes(vd_engine* e, const vd_batch* b, const vd_params* p, con
         if (out_certainty)
           for (int64_t k = 0; k < n_rows; ++k) out_certainty[row_read[k]] = cert[(size_t)k];
         s.kernel_ms += ms;
-        s.kernel_launches += 2;
+        s.kernel_launches += guard ? 3 : 2;
         s.d2h_bytes = gl_off[G] * 8 + (out_values ? n_out * 8 : 0) + (out_certainty ? n_rows * 8 : 0) +
-                      (out_ln ? n_out * 8 : 0);
+                      (out_ln ? n_out * 8 : 0) + (guard ? G * 4 : 0);
       }
     }
   }
   vd_plan_destroy(pl);
   if (rc) return rc;
+  if (out_guarded) for (int64_t g = 0; g < G; ++g) out_guarded[g] = flags[(size_t)g];
+
+  // near ties: the flagged regions again, in FP64, their results in place
+  std::vector<int64_t> tied;
+  for (int64_t g = 0; g < G; ++g) if (flags[(size_t)g]) tied.push_back(g);
+  if (!tied.empty()) {
+    std::vector<unsigned char> rb, rq, hb, mq;
+    std::vector<int64_t> ro{0}, ho{0}, rro{0}, rho{0};
+    for (int64_t g : tied) {
+      const int64_t r0 = b->region_read_off[g], r1 = b->region_read_off[g + 1];
+      const int64_t h0 = b->region_hap_off[g], h1 = b->region_hap_off[g + 1];
+      for (int64_t r = r0; r < r1; ++r) {
+        const int64_t a0 = b->read_off[r], a1 = b->read_off[r + 1];
+        rb.insert(rb.end(), b->read_bases + a0, b->read_bases + a1);
+        rq.insert(rq.end(), b->read_quals + a0, b->read_quals + a1);
+        ro.push_back(ro.back() + (a1 - a0));
+        mq.push_back(mapping_quality ? mapping_quality[r] : (unsigned char)60);
+      }
+      for (int64_t h = h0; h < h1; ++h) {
+        const int64_t c0 = b->hap_off[h], c1 = b->hap_off[h + 1];
+        hb.insert(hb.end(), b->hap_bases + c0, b->hap_bases + c1);
+        ho.push_back(ho.back() + (c1 - c0));
+      }
+      rro.push_back(rro.back() + (r1 - r0));
+      rho.push_back(rho.back() + (h1 - h0));
+    }
+    vd_batch sub{};
+    sub.read_bases = rb.data();
+    sub.read_quals = rq.data();
+    sub.read_off = ro.data();
+    sub.n_reads = (int64_t)ro.size() - 1;
+    sub.hap_bases = hb.data();
+    sub.hap_off = ho.data();
+    sub.n_haps = (int64_t)ho.size() - 1;
+    sub.region_read_off = rro.data();
+    sub.region_hap_off = rho.data();
+    sub.n_regions = (int64_t)tied.size();
+    vd_params p64 = *p;
+    p64.precision = VD_PRECISION_FLOAT64;
+    vd_genotype_options o64 = *opt;
+    o64.near_tie_guard = 0;
+    int64_t sub_out = 0, sub_gl = 0;
+    for (size_t k = 0; k < tied.size(); ++k) {
+      const int64_t g = tied[k], H = r_h[(size_t)g];
+      sub_out += r_reads[(size_t)g] * H;
+      sub_gl += H * (H + 1) / 2;
+    }
+    std::vector<double> ln2((size_t)sub_out), val2((size_t)sub_out), cert2((size_t)sub.n_reads), gl2((size_t)sub_gl);
+    vd_stats s2{};
+    rc = vd_region_genotypes(e, &sub, &p64, mq.data(), &o64, ln2.data(), val2.data(), cert2.data(), gl2.data(),
+                             nullptr, &s2);
+    if (rc) return rc;
+    int64_t so = 0, sg = 0, sr = 0;
+    for (int64_t g : tied) {
+      const int64_t H = r_h[(size_t)g], nr = r_reads[(size_t)g], P = H * (H + 1) / 2;
+      for (int64_t k = 0; k < nr * H; ++k) {
+        if (out_ln) out_ln[r_out[(size_t)g] + k] = ln2[(size_t)(so + k)];
+        if (out_values) out_values[r_out[(size_t)g] + k] = val2[(size_t)(so + k)];
+      }
+      for (int64_t k = 0; k < P; ++k) out_gl[gl_off[(size_t)g] + k] = gl2[(size_t)(sg + k)];
+      if (out_certainty)
+        for (int64_t k = 0; k < nr; ++k) out_certainty[b->region_read_off[g] + k] = cert2[(size_t)(sr + k)];
+      so += nr * H;
+      sg += P;
+      sr += nr;
+    }
+    s.kernel_ms += s2.kernel_ms;
+    s.kernel_launches += s2.kernel_launches;
+    s.rescued_fp64 += s2.pairs;
+  }
   s.total_ms = now_ms() - t0;
   if (st) *st = s;
   return VD_OK;

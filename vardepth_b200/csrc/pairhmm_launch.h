@@ -35,6 +35,8 @@ cudaError_t launch_genotype_gl(const double* values, const int64_t* region_out_o
                                const int32_t* region_h, const int64_t* gl_off, const int64_t* acc_off,
                                int64_t n_regions, double prior, double* acc, double* gl, int sm_count,
                                cudaStream_t stream);
+cudaError_t launch_genotype_ties(const double* gl, const int64_t* gl_off, const int32_t* region_h,
+                                 const int64_t* region_reads, int64_t n_regions, int* flags, cudaStream_t stream);
 // sets the message vd_last_error returns on this thread; returns code
 int report_error(int code, const char* msg);
 // model tables for (gap, ext, optional per-bin Phred offsets), built on the host

@@ -62,6 +62,10 @@ class VdTuning(ctypes.Structure):
                 "max_item_columns": self.max_item_columns}
 
 
+class VdGenotypeOptions(ctypes.Structure):
+    _fields_ = [("artifact_prior", ctypes.c_double), ("near_tie_guard", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+
+
 class VdGradStats(ctypes.Structure):
     _fields_ = [("pairs", c_i64), ("dp_cells", c_i64), ("fp64_pairs", c_i64), ("failed_pairs", c_i64),
                 ("scratch_bytes", c_i64), ("kernel_launches", c_i64), ("kernel_ms", ctypes.c_double),
@@ -78,8 +82,8 @@ SIGNATURES = {
     "vd_engine_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "vd_region_genotypes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams),
-                                           c_u8p, ctypes.c_double, c_dp, c_dp, c_dp, c_dp,
-                                           ctypes.POINTER(VdStats)]),
+                                           c_u8p, ctypes.POINTER(VdGenotypeOptions), c_dp, c_dp, c_dp, c_dp,
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(VdStats)]),
     "vd_engine_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdTuning)]),
     "vd_engine_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdTuning)]),
     "vd_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams), c_dp,
@@ -277,7 +281,8 @@ class Engine:
         return ln, jac, stats
 
     def region_genotypes(self, packed: Packed, params: VdParams, mapping_quality=None, artifact_prior=None,
-                         values: bool = True, certainty: bool = True, ln: bool = True) -> dict:
+                         values: bool = True, certainty: bool = True, ln: bool = True,
+                         near_tie_guard: bool = False) -> dict:
         """Forward pass plus on-device normalised rows and diploid genotype log-likelihoods of
         every region (vd_region_genotypes); ``gl`` is a list with one array per region."""
         if packed.pair_read is not None:
@@ -292,15 +297,21 @@ class Engine:
         mq = None if mapping_quality is None else np.ascontiguousarray(mapping_quality, np.uint8)
         if mq is not None and len(mq) != len(packed.read_off) - 1:
             raise ValueError("one mapping quality per read")
-        prior = -1.0 if artifact_prior is None else float(artifact_prior)
+        options = VdGenotypeOptions()
+        options.artifact_prior = -1.0 if artifact_prior is None else float(artifact_prior)
+        options.near_tie_guard = 1 if near_tie_guard else 0
+        guarded = np.zeros(len(P), np.int32)
         stats = VdStats()
         opt = lambda a: a.ctypes.data_as(c_dp) if a is not None else ctypes.cast(None, c_dp)
         check(library().vd_region_genotypes(self.handle, ctypes.byref(packed.batch), ctypes.byref(params),
-                                            _ptr(mq, ctypes.c_ubyte), prior, opt(out["ln"]), opt(out["values"]),
-                                            opt(out["certainty"]), gl.ctypes.data_as(c_dp), ctypes.byref(stats)),
+                                            _ptr(mq, ctypes.c_ubyte), ctypes.byref(options), opt(out["ln"]),
+                                            opt(out["values"]), opt(out["certainty"]), gl.ctypes.data_as(c_dp),
+                                            guarded.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                            ctypes.byref(stats)),
               "vd_region_genotypes")
         offs = np.concatenate([[0], np.cumsum(P)])
         out["gl"] = [gl[offs[g]:offs[g + 1]] for g in range(len(P))]
+        out["guarded"] = guarded.astype(bool)
         out["stats"] = stats
         return out
 
