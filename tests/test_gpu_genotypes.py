@@ -85,13 +85,14 @@ def test_mixed_precision_calls_and_optional_outputs(engine):
 
 
 def test_near_tie_guard_rescores_tied_regions_in_fp64(engine):
-    """partial_anchor.py:120-133 as a device flag: a region whose haplotypes are identical ties every
-    genotype and is rescored in FP64; a region with a clear call keeps its mixed-precision result."""
+    """partial_anchor.py:120-133 as a device flag: a region whose haplotypes are all identical ties
+    every genotype and is rescored in FP64; a region with a clear call keeps its mixed-precision result."""
     w = S.config1(n_regions=6, seed=21)
-    # region 0 gets two copies of its first haplotype
+    # every haplotype of region 0 is a copy of its first: all its genotypes tie
     haps = [w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]] for h in range(len(w.hap_off) - 1)]
     h0 = w.region_hap_off[0]
-    haps[h0 + 1] = haps[h0].copy()
+    for h in range(h0 + 1, w.region_hap_off[1]):
+        haps[h] = haps[h0].copy()
     hap_bases = np.concatenate(haps)
     hap_off = np.concatenate([[0], np.cumsum([len(h) for h in haps])])
     pk = native.Packed(w.read_bases, w.read_quals, w.read_off, hap_bases, hap_off,

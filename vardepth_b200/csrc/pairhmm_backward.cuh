@@ -33,11 +33,13 @@
 // Memory: the forward values a backward step needs (mu and omega of the
 // lane's rows and the u handed in from the row above: 2R+1 values per lane
 // and step) are produced by recomputation.  A first forward pass stores the
-// warp state every C steps (C = ceil(sqrt(T)) for T = m + 32 steps, "sqrt-L
-// anti-diagonal checkpointing"); the reverse sweep then replays each segment
-// of C steps from its checkpoint into a segment buffer and walks it back.
-// With store_all the first pass keeps every step (one segment of T steps).
-// Both give bit-identical results.
+// warp state every C steps (C = ceil(sqrt(T)) for T = m + 33 steps, "sqrt-L
+// anti-diagonal checkpointing"); the reverse sweep replays each segment of C
+// steps from its checkpoint once to lay down a state every kSub = 8 steps,
+// then replays each 8-step sub-segment into a shared-memory buffer and walks
+// it back from there, so the per-step values never leave the SM.  With
+// store_all the first pass keeps every step in global memory (one segment of
+// T steps).  Both give bit-identical results.
 #pragma once
 #include "pairhmm_kernel.cuh"
 
@@ -82,13 +84,22 @@ __host__ __device__ inline int grad_interval(int steps, bool store_all) {
   int c = (int)ceil(sqrt((double)steps));
   return c < 4 ? 4 : c;
 }
-// Elements of type T one warp slot needs for a pair with R rows per lane.
+// Steps of the shared-memory sub-segment buffer (sqrt-L mode): each sqrt(T)
+// segment is replayed once to lay down a warp state every kSub steps, then
+// sub-segment by sub-segment into shared memory and walked back from there.
+constexpr int kSub = 8;
+// Shared memory of one warp's sub-segment buffer, sized for R = 8.
+template <typename T>
+__host__ __device__ constexpr int grad_smem_per_warp() { return kSub * (2 * kMaxR + 1) * kWarp * (int)sizeof(T); }
+// Elements of type T one warp slot needs in global memory for a pair with R
+// rows per lane: the sqrt(T) checkpoints and the sub-segment states, or every
+// step's buffer row when store_all.
 __host__ __device__ inline long long grad_slot_elems(int R, int m, bool store_all) {
   const int steps = grad_steps(m);
   const int C = grad_interval(steps, store_all);
   const int nseg = (steps + C - 1) / C;
-  const long long ck = store_all ? 0 : (long long)nseg * (3 * R + 2) * kWarp;
-  return ck + (long long)C * (2 * R + 1) * kWarp;
+  if (store_all) return (long long)C * (2 * R + 1) * kWarp;
+  return ((long long)nseg + (C + kSub - 1) / kSub) * (3 * R + 2) * kWarp;
 }
 
 // The adjoint starts at rho = 2^k on the last row, with rho Zs near 2^kTarget
@@ -103,7 +114,7 @@ template <typename T, int R, bool GEN>
 __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, const RescueEntry item,
                                        const Tables<T>* __restrict__ tb, const Scalars<T>& sc,
                                        const GradTables* __restrict__ gt, const GradScalars& gs, const int lane,
-                                       T* __restrict__ slot) {
+                                       T* __restrict__ slot, T* __restrict__ sbuf) {
   constexpr unsigned FULL = 0xffffffffu;
   const int64_t roff = bv.read_off[item.read];
   const int n = (int)(bv.read_off[item.read + 1] - roff);
@@ -120,8 +131,9 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   const int nseg = (steps + C - 1) / C;
   constexpr int CKW = 3 * R + 2;  // checkpoint words per lane
   constexpr int BFW = 2 * R + 1;  // segment-buffer words per lane and step
-  T* __restrict__ ck = slot;
-  T* __restrict__ buf = slot + (store_all ? 0 : (long long)nseg * CKW * kWarp);
+  T* __restrict__ ck = slot;                                   // sqrt(T) checkpoints
+  T* __restrict__ sub = slot + (long long)nseg * CKW * kWarp;   // states every kSub steps of a segment
+  T* __restrict__ buf = slot;                                  // store_all: every step
 
   const T k2 = sc.k2, x = sc.x, c0 = sc.c;
   const T A = tb->A[rqual[n - 1]];
@@ -152,8 +164,9 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   T s_top = T(0), u_bot = T(0);
   double acc = 0.0;
 
-  // one forward step; with rec the lane's column values go to buffer row t - t0
-  auto fstep = [&](const int t, const int t0, const bool rec) {
+  // one forward step; with rec the lane's column values go to row t - t0 of
+  // dst (the global buffer, or this warp's shared sub-segment buffer)
+  auto fstep = [&](const int t, const int t0, const bool rec, T* __restrict__ dst) {
     const int j = t - lane;
     T u_in = __shfl_up_sync(FULL, u_bot, 1);
     T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
@@ -169,7 +182,7 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     column<T, R, GEN, false>(rw, hb, s_top, u_in, k2, x, u_bot, d0, d1, d2);
     s_top = s_in;
     if (rec && act) {
-      T* e = buf + (long long)(t - t0) * BFW * kWarp + lane;
+      T* e = dst + (long long)(t - t0) * BFW * kWarp + lane;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         e[r * kWarp] = rw.mu[r];
@@ -179,8 +192,8 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     }
     if (lane == kWarp - 1 && act) acc += (double)u_bot;
   };
-  auto save_state = [&](const int k) {
-    T* e = ck + (long long)k * CKW * kWarp + lane;
+  auto save_state = [&](T* __restrict__ area, const int k) {
+    T* e = area + (long long)k * CKW * kWarp + lane;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       e[r * kWarp] = rw.mu[r];
@@ -190,8 +203,8 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     e[3 * R * kWarp] = s_top;
     e[(3 * R + 1) * kWarp] = u_bot;
   };
-  auto load_state = [&](const int k) {
-    const T* e = ck + (long long)k * CKW * kWarp + lane;
+  auto load_state = [&](const T* __restrict__ area, const int k) {
+    const T* e = area + (long long)k * CKW * kWarp + lane;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       rw.mu[r] = e[r * kWarp];
@@ -204,8 +217,8 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
 
   // ---- first forward pass: Zs, and the checkpoints (or every step) ----
   for (int t = 0; t < steps; ++t) {
-    if (!store_all && t % C == 0) save_state(t / C);
-    fstep(t, 0, store_all);
+    if (!store_all && t % C == 0) save_state(ck, t / C);
+    fstep(t, 0, store_all, buf);
   }
   const double Zs = __shfl_sync(FULL, acc, kWarp - 1);
   double lnN = 0.0;
@@ -242,7 +255,7 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   T Bk2 = T(0), Ax = T(0);
   T top_u = T(0), top_s = T(0), pend_s = T(0);
 
-  auto bstep = [&](const int t, const int t0) {
+  auto bstep = [&](const int t, const int t0, const T* __restrict__ src) {
     const int j = t - lane;
     const bool act = (unsigned)j <= (unsigned)m;
     T in_u = __shfl_down_sync(FULL, top_u, 1);
@@ -255,7 +268,7 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
       top_s = T(0);
       return;
     }
-    const T* e = buf + (long long)(t - t0) * BFW * kWarp + lane;
+    const T* e = src + (long long)(t - t0) * BFW * kWarp + lane;
     T muf[R], omf[R], nu[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -295,16 +308,32 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     top_s = ups[0];
   };
 
-  for (int k = nseg - 1; k >= 0; --k) {
-    const int t0 = k * C;
-    const int t1 = min(steps, t0 + C);
-    if (!store_all) {
-      load_state(k);
-      for (int t = t0; t < t1; ++t) fstep(t, t0, true);
+  if (store_all) {
+    __syncwarp();
+    for (int t = steps - 1; t >= 0; --t) bstep(t, 0, buf);
+    __syncwarp();
+  } else {
+    for (int k = nseg - 1; k >= 0; --k) {
+      const int t0 = k * C;
+      const int t1 = min(steps, t0 + C);
+      // lay down a state every kSub steps of the segment, then walk the
+      // sub-segments back through shared memory
+      load_state(ck, k);
+      for (int t = t0; t < t1; ++t) {
+        if ((t - t0) % kSub == 0) save_state(sub, (t - t0) / kSub);
+        fstep(t, t0, false, buf);
+      }
+      __syncwarp();
+      for (int q = (t1 - t0 - 1) / kSub; q >= 0; --q) {
+        const int ta = t0 + q * kSub;
+        const int tb = min(t1, ta + kSub);
+        load_state(sub, q);
+        for (int t = ta; t < tb; ++t) fstep(t, ta, true, sbuf);
+        __syncwarp();
+        for (int t = tb - 1; t >= ta; --t) bstep(t, ta, sbuf);
+        __syncwarp();
+      }
     }
-    __syncwarp();
-    for (int t = t1 - 1; t >= t0; --t) bstep(t, t0);
-    __syncwarp();
   }
 
   // ---- chain rule to theta (FP64) ----
@@ -374,9 +403,11 @@ pairhmm_grad_kernel(const BatchView bv, const GradView gv, const Tables<T>* __re
     for (int i = threadIdx.x; i < gwords; i += blockDim.x) gdst[i] = gsrc[i];
   }
   __syncthreads();
+  extern __shared__ __align__(16) unsigned char grad_dyn[];
   const int lane = threadIdx.x & (kWarp - 1);
   const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   T* slot = reinterpret_cast<T*>(gv.scratch + gw * gv.slot_bytes);
+  T* sbuf = reinterpret_cast<T*>(grad_dyn + (threadIdx.x >> 5) * grad_smem_per_warp<T>());
   long long total = gv.n_items;
   if (gv.count != nullptr) {
     const long long c = (long long)*gv.count;
@@ -392,8 +423,8 @@ pairhmm_grad_kernel(const BatchView bv, const GradView gv, const Tables<T>* __re
     const bool gen = code_general(code);
 #define VD_GCASE(r)                                                                          \
   case r:                                                                                    \
-    if (gen) grad_pair<T, r, true>(bv, gv, item, &tab, sc, &gt, gs, lane, slot);           \
-    else grad_pair<T, r, false>(bv, gv, item, &tab, sc, &gt, gs, lane, slot);              \
+    if (gen) grad_pair<T, r, true>(bv, gv, item, &tab, sc, &gt, gs, lane, slot, sbuf);     \
+    else grad_pair<T, r, false>(bv, gv, item, &tab, sc, &gt, gs, lane, slot, sbuf);        \
     break;
     switch (code_R(code)) {
       VD_GCASE(1) VD_GCASE(2) VD_GCASE(3) VD_GCASE(4) VD_GCASE(5) VD_GCASE(6) VD_GCASE(7) VD_GCASE(8)
