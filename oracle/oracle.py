@@ -199,13 +199,15 @@ def diploid_gl(v, artifact_prior=None):
     a, b = np.array([(a, b) for b in range(H) for a in range(b + 1)]).T
     va, vb = v[:, a], v[:, b]
     if artifact_prior is None:
+        # numpy's maximum keeps NaN (rows of an empty read)
         return np.log(np.maximum(1e-300, (va + vb) / 2)).sum(axis=0)
-    clean = np.array([np.log(np.maximum(1e-300, w * va + (1 - w) * vb)).sum(axis=0) + np.log(q)
+    # the C++ mixture's std::max(1e-300, x) turns NaN into 1e-300, as np.fmax does
+    clean = np.array([np.log(np.fmax(1e-300, w * va + (1 - w) * vb)).sum(axis=0) + np.log(q)
                       for w, q in zip(_BALANCE, _BALANCE_W)])
     clean = np.logaddexp.reduce(clean, axis=0)
     if artifact_prior <= 0:
         return clean
-    art = [np.log(np.maximum(1e-300, (1 - t) * (va + vb) / 2 + t * v[:, c, None])).sum(axis=0) + np.log(q / H)
+    art = [np.log(np.fmax(1e-300, (1 - t) * (va + vb) / 2 + t * v[:, c, None])).sum(axis=0) + np.log(q / H)
            for t, q in zip(_THETA, _THETA_W) for c in range(H)]
     art = np.logaddexp.reduce(np.array(art), axis=0)
     return np.logaddexp(np.log1p(-artifact_prior) + clean, np.log(artifact_prior) + art)

@@ -110,3 +110,29 @@ def test_near_tie_guard_rescores_tied_regions_in_fp64(engine):
     nr, H = int(w.region_read_off[1]), int(w.region_hap_off[1])
     np.testing.assert_array_equal(guarded["ln"][:nr * H], exact["ln"][:nr * H])
     np.testing.assert_array_equal(guarded["certainty"][:nr], exact["certainty"][:nr])
+
+
+@pytest.mark.parametrize("prior", [None, 0.0, 0.01])
+def test_edge_regions(engine, prior):
+    """Regions with one haplotype, with no reads, and with an empty read, against the oracle."""
+    rng = np.random.default_rng(4)
+    hap = S.ALPHABET[rng.integers(0, 4, 90)]
+    reads = [hap[10:60], hap[30:80], np.empty(0, np.uint8), hap[5:45]]
+    rb = np.concatenate(reads)
+    rq = np.full(len(rb), 30, np.uint8)
+    ro = np.concatenate([[0], np.cumsum([len(r) for r in reads])])
+    haps = [hap, hap[:70], hap[20:], hap]
+    hb = np.concatenate(haps)
+    ho = np.concatenate([[0], np.cumsum([len(h) for h in haps])])
+    # region 0: reads 0-1 x hap 0 (H = 1); region 1: no reads x haps 1-2; region 2: reads 2-3 x haps 2-3
+    rro, rho = [0, 2, 2, 4], [0, 1, 3, 4]
+    pk = native.Packed(rb, rq, ro, hb, ho, region_read_off=rro, region_hap_off=rho)
+    params, _ = native.make_params(0.001, 0.1, False, native.VD_PRECISION_FLOAT64)
+    mq = np.array([60, 20, 60, 5], np.uint8)
+    res = engine.region_genotypes(pk, params, mq, prior)
+    assert [len(g) for g in res["gl"]] == [1, 3, 1]
+    np.testing.assert_allclose(res["gl"][1], np.zeros(3), atol=1e-15)
+    v, c, gl = _oracle_post(res["ln"], np.array(rro), np.array(rho), mq, prior)
+    for a, b in zip(res["gl"], gl):
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12)
+    assert np.isneginf(res["ln"][2]) and np.isnan(res["certainty"][2]) == np.isnan(c[2])

@@ -105,8 +105,13 @@ __global__ void gl_kernel(const double* __restrict__ values, const int64_t* __re
       const int ia = p - b * (b + 1) / 2, ib = b;
       double s = 0.0;
       if (prior < 0.0) {
-        for (int64_t r = 0; r < R; ++r) s += log(fmax(1e-300, (v[r * H + ia] + v[r * H + ib]) / 2));
+        // numpy's maximum (triangular.py:16) keeps a NaN row (an empty read) as NaN
+        for (int64_t r = 0; r < R; ++r) {
+          const double t = (v[r * H + ia] + v[r * H + ib]) / 2;
+          s += log(t != t ? t : fmax(1e-300, t));
+        }
       } else if (j < 7) {
+        // std::max(1e-300, x) of mixture_general.cpp:22-24 turns NaN into 1e-300 (fmax does too)
         const double w = c_balance[j];
         for (int64_t r = 0; r < R; ++r) s += log(fmax(1e-300, w * v[r * H + ia] + (1 - w) * v[r * H + ib]));
       } else {

@@ -171,7 +171,7 @@ struct vd_engine {
   cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
   std::mutex mu;
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
-  int grid_pair = 0;                  // blocks of the two-read kernel
+  int grid_pair[2] = {0, 0};          // blocks of the two-read kernels [wide]
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
   vd_tuning tuning{256, 0x1fe, 0, {0, 0, 0, 0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
@@ -327,7 +327,8 @@ struct HostChunk {
   int max_hap = 0;
   bool any_long = false;           // a read longer than 32 (the robust tier strip-mines it)
   bool any_strip = false;          // a read longer than one 256-row strip (every tier strip-mines it)
-  int64_t n_paired = 0;            // leading items that carry two reads (own kernel)
+  int64_t n_paired = 0;            // leading items that carry two reads (own kernels)
+  int64_t n_paired_wide = 0;       // the first of them, with 6-8 rows per lane
 };
 
 // The robust tier runs on a small grid: it only sees pairs the FP64 wavefront
@@ -564,6 +565,8 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   auto mid = std::stable_partition(c.items.begin(), c.items.end(),
                                    [](const WorkItem& w) { return code_paired(w.code); });
   c.n_paired = (int64_t)(mid - c.items.begin());
+  auto wide = std::stable_partition(c.items.begin(), mid, [](const WorkItem& w) { return code_R(w.code) >= 6; });
+  c.n_paired_wide = (int64_t)(wide - c.items.begin());
 }
 
 // Pair form: pairs grouped by read (counting sort), each read's haplotypes as
@@ -826,13 +829,17 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   int n = 0;
   if (!pl->chunk.items.empty()) {
     cudaError_t err = cudaSuccess;
-    const int64_t np = pl->chunk.n_paired;
-    if (np > 0) {
-      // two-read items first, on their own kernel (FP32 semiglobal only)
+    const int64_t np = pl->chunk.n_paired, nw = pl->chunk.n_paired_wide;
+    // two-read items first, on their own kernels (FP32 semiglobal only):
+    // 6-8 rows per lane, then up to 5
+    for (int k = 0; k < 2; ++k) {
+      const int64_t lo = k ? nw : 0, hi = k ? np : nw;
+      if (hi <= lo) continue;
       QueueView qp = q;
-      qp.n_items = np;
-      qp.head = cnt + 6;
-      err = launch_pair_f32(bv, qp, &dt->f32, ht->s32, e->grid_pair, pl->stream);
+      qp.items = (const WorkItem*)(d + L.o_items) + lo;
+      qp.n_items = hi - lo;
+      qp.head = cnt + 6 + k;
+      err = launch_pair_f32(k == 0, bv, qp, &dt->f32, ht->s32, e->grid_pair[k == 0 ? 1 : 0], pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "two-read tier launch");
       ++n;
     }
@@ -928,9 +935,13 @@ int init_engine_grids(vd_engine* e) {
       e->grid[f][a] = std::max(1, bps) * e->sm_count;
     }
   int bps = 0;
-  cudaError_t err = occupancy_pair_f32(&bps);
-  if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
-  e->grid_pair = std::max(1, bps) * e->sm_count;
+  cudaError_t err = cudaSuccess;
+  for (int wide = 0; wide < 2; ++wide) {
+    bps = 0;
+    err = occupancy_pair_f32(wide != 0, &bps);
+    if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+    e->grid_pair[wide] = std::max(1, bps) * e->sm_count;
+  }
   for (int f = 0; f < 2; ++f) {
     bps = 0;
     err = occupancy_grad(f != 0, &bps);

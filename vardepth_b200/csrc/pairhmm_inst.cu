@@ -36,15 +36,18 @@ cudaError_t VD_NAME(occupancy, VD_TNAME, VD_MNAME)(int* blocks_per_sm) {
 }
 
 #if !VD_FP64 && !VD_ANCH
-cudaError_t launch_pair_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
+cudaError_t launch_pair_f32(bool wide, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                             const Scalars<float>& sc, int grid, cudaStream_t stream) {
-  pairhmm_pair_kernel<0><<<grid, kWarpsPerBlock * kWarp, 0, stream>>>(bv, qv, tab, sc);
+  if (wide) pairhmm_pair_kernel<6, 8, 3><<<grid, kWarpsPerBlock * kWarp, 0, stream>>>(bv, qv, tab, sc);
+  else pairhmm_pair_kernel<1, 5, 4><<<grid, kWarpsPerBlock * kWarp, 0, stream>>>(bv, qv, tab, sc);
   return cudaGetLastError();
 }
 
-cudaError_t occupancy_pair_f32(int* blocks_per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<0>,
-                                                       kWarpsPerBlock * kWarp, 0);
+cudaError_t occupancy_pair_f32(bool wide, int* blocks_per_sm) {
+  return wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<6, 8, 3>,
+                                                              kWarpsPerBlock * kWarp, 0)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<1, 5, 4>,
+                                                              kWarpsPerBlock * kWarp, 0);
 }
 #endif
 

@@ -91,7 +91,7 @@ __device__ __forceinline__ void spill_pair(const QueueView& qv, int32_t read, in
   }
 }
 
-constexpr int kUnroll = 4;
+constexpr int kUnroll = 8;
 
 // Row layout of one read (lane L, register r of strip s holds row
 // i = s*32R + L*R + r - v, 0-based):
@@ -707,11 +707,13 @@ pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restri
   }
 }
 
-// Persistent kernel of the two-read items (FP32, semiglobal).  Its packed
-// rows need about 14 registers each, so it runs 3 blocks per SM on its own
-// work list, ahead of the single-read items of the same tier.
-template <int kUnused = 0>
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, 3)
+// Persistent kernels of the two-read items (FP32, semiglobal), on their own
+// work list ahead of the single-read items of the same tier.  Packed rows
+// need about 14 registers each: items with 6-8 rows per lane run 3 blocks per
+// SM (168 registers), items with up to 5 rows 4 blocks (128 registers), each
+// kernel instantiating only its own row counts.
+template <int kLoR, int kHiR, int kBlocks>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
 pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
                     const Scalars<float> sc) {
   __shared__ Tables<float> tab;
@@ -733,14 +735,10 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
     it.use_sel = false;
     it.tier = 0;
     switch (code_R(it.w.code)) {
-      case 1: process_pair<1>(bv, qv, it, &tab, sc, lane); break;
-      case 2: process_pair<2>(bv, qv, it, &tab, sc, lane); break;
-      case 3: process_pair<3>(bv, qv, it, &tab, sc, lane); break;
-      case 4: process_pair<4>(bv, qv, it, &tab, sc, lane); break;
-      case 5: process_pair<5>(bv, qv, it, &tab, sc, lane); break;
-      case 6: process_pair<6>(bv, qv, it, &tab, sc, lane); break;
-      case 7: process_pair<7>(bv, qv, it, &tab, sc, lane); break;
-      case 8: process_pair<8>(bv, qv, it, &tab, sc, lane); break;
+#define VD_PCASE(r) \
+      case r: if constexpr (r >= kLoR && r <= kHiR) process_pair<r>(bv, qv, it, &tab, sc, lane); break;
+      VD_PCASE(1) VD_PCASE(2) VD_PCASE(3) VD_PCASE(4) VD_PCASE(5) VD_PCASE(6) VD_PCASE(7) VD_PCASE(8)
+#undef VD_PCASE
       default: break;
     }
   }

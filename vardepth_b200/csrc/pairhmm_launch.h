@@ -10,10 +10,10 @@ cudaError_t launch_f64(bool anchored, const BatchView& bv, const QueueView& qv, 
                        const Scalars<double>& sc, int tier, int grid, cudaStream_t stream);
 cudaError_t occupancy_f32(bool anchored, int* blocks_per_sm);
 cudaError_t occupancy_f64(bool anchored, int* blocks_per_sm);
-// two-read items (FP32, semiglobal)
-cudaError_t launch_pair_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
+// two-read items (FP32, semiglobal): wide = 6-8 rows per lane, else 1-5
+cudaError_t launch_pair_f32(bool wide, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                             const Scalars<float>& sc, int grid, cudaStream_t stream);
-cudaError_t occupancy_pair_f32(int* blocks_per_sm);
+cudaError_t occupancy_pair_f32(bool wide, int* blocks_per_sm);
 // gradient kernel (pairhmm_backward.cuh), FP32 and FP64 passes
 struct GradTables;
 struct GradScalars;
