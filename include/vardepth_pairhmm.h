@@ -194,7 +194,10 @@ double vd_anchored_pairhmm(const char *read, const unsigned char *qual, int n, c
  * precision = VD_PRECISION_FLOAT64).  Memory: VD_CHECKPOINT_SQRT keeps the
  * warp state every ceil(sqrt(T)) anti-diagonals (T = m + 33) and replays one
  * segment at a time; VD_CHECKPOINT_ALL keeps every anti-diagonal.  Both give
- * identical results.  Reads of at most 256 bases; anchored = 0; gap, ext > 0.
+ * identical results.  Semiglobal and anchored models; reads of at most 256
+ * bases (255 anchored); gap, ext > 0.  In anchored mode the gradient is that of
+ * the end cell without the 1e-300 floor of anchored.cpp:24 (which binds only
+ * for end cells 1e-300 below the last row's maximum).
  * out_ln and out_jac (6 doubles per output) are host arrays in the output
  * order of vd_forward.  Empty reads or haplotypes give -inf and a zero row. */
 enum { VD_CHECKPOINT_SQRT = 0, VD_CHECKPOINT_ALL = 1 };

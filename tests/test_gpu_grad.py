@@ -130,6 +130,54 @@ def test_low_qualities_two_sided_rows_and_floor(engine):
         assert np.all(np.abs(jac - jo) <= 1e-4 * np.maximum(np.abs(jo), 1e-2))
 
 
+def _anchored_windows(seed, sites=12, reads=10):
+    """Read spans against haplotype windows of about their length, as indel refinement scores them
+    (caller/native/caller/indel_refine.py:143-151)."""
+    rng = np.random.default_rng(seed)
+    rb, rq, hb, ro, ho = [], [], [], [0], [0]
+    for _ in range(sites):
+        ref = S.ALPHABET[rng.integers(0, 4, 300)]
+        p, k = int(rng.integers(120, 180)), int(rng.integers(1, 8))
+        alt = np.concatenate([ref[:p], ref[p + k:]]) if rng.random() < 0.5 else \
+            np.concatenate([ref[:p], S.ALPHABET[rng.integers(0, 4, k)], ref[p:]])
+        for _ in range(reads):
+            src = alt if rng.random() < 0.5 else ref
+            a, b = int(rng.integers(10, 80)), int(rng.integers(p + 20, p + 110))
+            read = src[a:b].copy()
+            flip = rng.random(len(read)) < 0.02
+            read[flip] = S.ALPHABET[(np.searchsorted(S.ALPHABET, read[flip]) + 1) % 4]
+            for hap in (ref, alt):
+                rb.append(read)
+                rq.append(rng.choice([10, 20, 30, 40], len(read), p=[.05, .15, .5, .3]).astype(np.uint8))
+                ro.append(ro[-1] + len(read))
+                w = hap[a:b + len(hap) - len(src)]
+                hb.append(w)
+                ho.append(ho[-1] + len(w))
+    idx = np.arange(len(rb), dtype=np.int32)
+    return np.concatenate(rb), np.concatenate(rq), np.array(ro), np.concatenate(hb), np.array(ho), idx
+
+
+def test_anchored_jacobian(engine):
+    """The anchored (global) model: ln L of the end cell and its gradient, with the row-0 emulator."""
+    rb, rq, ro, hb, ho, idx = _anchored_windows(3)
+    pk = native.Packed(rb, rq, ro, hb, ho, pair_read=idx, pair_hap=idx)
+    g, x = O.phred_to_prob(THETA[0]), O.phred_to_prob(THETA[1])
+    lo, jo = O.grad_pairs(rb, rq, ro, hb, ho, idx, idx, g, x, True, THETA[2:])
+    p64, _ = native.make_params(g, x, True, native.VD_PRECISION_FLOAT64, quality_offsets=THETA[2:])
+    ln64, jac64, _ = engine.forward_backward(pk, p64)
+    np.testing.assert_allclose(ln64, lo, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(jac64, jo, rtol=1e-9, atol=1e-10)
+    pm, _ = native.make_params(g, x, True, native.VD_PRECISION_MIXED, quality_offsets=THETA[2:])
+    ln, jac, st = engine.forward_backward(pk, pm)
+    assert np.max(np.abs(ln - lo)) / LN10 <= 1e-4
+    total, want = jac.sum(0), jo.sum(0)
+    assert np.all(np.abs(total - want) <= 1e-6 * np.abs(want)), (total, want)
+    fw, _ = engine.forward(pk, pm)
+    assert np.max(np.abs(ln - fw)) / LN10 <= 1e-6
+    every = engine.forward_backward(pk, pm, native.VD_CHECKPOINT_ALL)
+    np.testing.assert_array_equal(every[1], jac)
+
+
 def test_empty_inputs_and_argument_errors(engine):
     rb = np.frombuffer(b"ACGTACGT", np.uint8)
     rq = np.full(8, 30, np.uint8)
@@ -144,7 +192,10 @@ def test_empty_inputs_and_argument_errors(engine):
         _fb(engine, long_read, THETA)
     params, _keep = native.make_params(0.001, 0.1, True, native.VD_PRECISION_MIXED)
     with pytest.raises(ValueError):
-        engine.forward_backward(pk, params)
+        engine.forward_backward(long_read, params)
+    ok = native.Packed(np.full(255, 65, np.uint8), np.full(255, 30, np.uint8), [0, 255], hb, [0, 10],
+                       region_read_off=[0, 1], region_hap_off=[0, 1])
+    engine.forward_backward(ok, params)  # 255 bases + the row-0 emulator fill one strip
 
 
 def test_autograd_backward_is_grad_output_times_jacobian(engine):

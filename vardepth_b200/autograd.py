@@ -30,12 +30,12 @@ THETA_NAMES = ("gap_open_phred", "gap_continuation_phred", "offset_q_lt15", "off
                "offset_q_ge35")
 
 
-def params_from_theta(theta: np.ndarray, precision: int = native.VD_PRECISION_MIXED):
+def params_from_theta(theta: np.ndarray, precision: int = native.VD_PRECISION_MIXED, anchored: bool = False):
     """vd_params for theta = (Qg, Qx, o0..o3)."""
     t = np.asarray(theta, np.float64)
     if t.shape != (6,):
         raise ValueError("theta must hold 6 values (Qg, Qx, o0, o1, o2, o3)")
-    return native.make_params(10.0 ** (-t[0] / 10.0), 10.0 ** (-t[1] / 10.0), False, precision,
+    return native.make_params(10.0 ** (-t[0] / 10.0), 10.0 ** (-t[1] / 10.0), anchored, precision,
                               quality_offsets=t[2:6])
 
 
@@ -43,21 +43,22 @@ class Batch:
     """A packed region or pair batch bound to an engine, for repeated likelihood calls."""
 
     def __init__(self, engine: native.Engine, packed: native.Packed, precision: int = native.VD_PRECISION_MIXED,
-                 checkpoint: int = native.VD_CHECKPOINT_SQRT):
+                 checkpoint: int = native.VD_CHECKPOINT_SQRT, anchored: bool = False):
         self.engine = engine
         self.packed = packed
         self.precision = precision
         self.checkpoint = checkpoint
+        self.anchored = anchored
         self.last_stats = None
 
     def loglik(self, theta: np.ndarray) -> np.ndarray:
-        params, _keep = params_from_theta(theta, self.precision)
+        params, _keep = params_from_theta(theta, self.precision, self.anchored)
         out, st = self.engine.forward(self.packed, params)
         self.last_stats = st
         return out
 
     def loglik_and_jacobian(self, theta: np.ndarray):
-        params, _keep = params_from_theta(theta, self.precision)
+        params, _keep = params_from_theta(theta, self.precision, self.anchored)
         ln, jac, st = self.engine.forward_backward(self.packed, params, self.checkpoint)
         self.last_stats = st
         return ln, jac

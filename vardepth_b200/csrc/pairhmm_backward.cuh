@@ -5,7 +5,7 @@
 // Phred Qx, Phred offsets o0..o3 of the four quality bins), g = 10^(-Qg/10),
 // x = 10^(-Qx/10), e = 10^(-max(0, min(q,60) + o_bin(q))/10).  The reference
 // has no differentiable PairHMM: this is reverse-mode differentiation of the
-// scaled forward recurrence of pairhmm_core.cuh (semiglobal mode), i.e. of
+// scaled forward recurrence of pairhmm_core.cuh, i.e. (semiglobal mode) of
 //   mu_i(j) = s_{i-1}(j-1) h_ij                 h = hit or miss of row i
 //   om_i(j) = mu_i(j-1) + x om_i(j-1)
 //   u_i(j)  = mu_i(j) + X_i u_{i-1}(j)          (X_n = A_n on the last row)
@@ -23,6 +23,10 @@
 // so that with the log-derivative tables of the constants (GradTables)
 //   d ln L = [sum_rows (X pu dlnX + K ps dlnK + bM dlnmiss + bH dlnhit)
 //             + k2 Bk2 dlnk2 + Ax dx] / (rho Zs) + sum_rows dlnN.
+// Anchored mode differentiates Zs = (mu + A nu + g om)_n(m), the end cell, with
+// the virtual row-0 emulator of the forward kernel; the end cell seeds the
+// adjoint (mu~ = rho, om~ = rho g, and rho A into u~ of the row above) and A
+// and g collect rho A nu and rho g om there.
 //
 // Layout: one warp per pair, lane L owns R consecutive rows (reads of at
 // most 256 bases, one strip), the anti-diagonal sweep of the forward kernel.
@@ -56,7 +60,7 @@ struct GradTables {
 
 // Derivatives with respect to Qg and Qx, identical for every row.
 struct GradScalars {
-  double dlnN_g, dlnK_g, dlnX_g, dlnA_g, dlnk2_g;
+  double dlnN_g, dlnK_g, dlnX_g, dlnA_g, dlnk2_g, dlng_g;
   double dlnK_x, dlnX_x, dlnk2_x, dx_x;
 };
 
@@ -70,6 +74,7 @@ struct GradView {
   char* scratch;                     // per warp slot: checkpoints and the segment buffer
   long long slot_bytes;
   int store_all;
+  int anchored;                      // 0: semiglobal, 1: anchored (global) model
   RescueEntry* spill;                // FP32 pass: pairs left to the FP64 pass
   unsigned long long* spill_count;
   long long spill_cap;
@@ -110,7 +115,7 @@ __host__ __device__ inline long long grad_slot_elems(int R, int m, bool store_al
 template <typename T> struct GradConsts { static constexpr int kTarget = 100, kMax = 120; };
 template <> struct GradConsts<double> { static constexpr int kTarget = 600, kMax = 900; };
 
-template <typename T, int R, bool GEN>
+template <typename T, int R, bool GEN, bool ANCH>
 __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, const RescueEntry item,
                                        const Tables<T>* __restrict__ tb, const Scalars<T>& sc,
                                        const GradTables* __restrict__ gt, const GradScalars& gs, const int lane,
@@ -135,27 +140,34 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   T* __restrict__ sub = slot + (long long)nseg * CKW * kWarp;   // states every kSub steps of a segment
   T* __restrict__ buf = slot;                                  // store_all: every step
 
-  const T k2 = sc.k2, x = sc.x, c0 = sc.c;
+  const T k2 = sc.k2, x = sc.x, c0 = sc.c, gfin = sc.gfin;
   const T A = tb->A[rqual[n - 1]];
 
-  // rows of this lane (the semiglobal layout of process_item, one strip)
+  // rows of this lane: the layout of process_item for one strip.  Semiglobal:
+  // row i = 32 lane ... with padding rows below the read passing u down.
+  // Anchored: the read is bottom-aligned below v = 32 R - n virtual rows, the
+  // lowest of them (i = -1) the emulator of row 0, fed s(-1) = c at column 0.
+  const int v = ANCH ? kWarp * R - n : 0;
+  int emu = -1;
   LaneRows<T, R, GEN> rw;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int i = lane * R + r;
-    if (i < n) {
+    const int i = lane * R + r - v;
+    if (i >= 0 && i < n) {
       const unsigned q = rqual[i];
       rw.rb[r] = rbase[i];
       rw.miss[r] = tb->miss[q];
       if (GEN) rw.hit[r] = tb->hit[q];
       rw.K[r] = tb->K[q];
-      rw.X[r] = (i == n - 1) ? A : tb->X[q];
+      rw.X[r] = (!ANCH && i == n - 1) ? A : tb->X[q];
     } else {
+      const bool emulator = ANCH && i == -1;
+      if (emulator) emu = r;
       rw.rb[r] = kNeverBase;
-      rw.miss[r] = T(0);
-      if (GEN) rw.hit[r] = T(0);
+      rw.miss[r] = emulator ? T(1) : T(0);
+      if (GEN) rw.hit[r] = rw.miss[r];
       rw.K[r] = T(0);
-      rw.X[r] = T(1);
+      rw.X[r] = (!ANCH && i >= n) ? T(1) : T(0);
     }
     rw.mu[r] = T(0);
     rw.om[r] = T(0);
@@ -163,6 +175,10 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   }
   T s_top = T(0), u_bot = T(0);
   double acc = 0.0;
+  // anchored end cell: (M + I + D)[n][m] = mu + A nu + g om of the last row at
+  // column m, the running maximum of that sum over the row (the 1e-300 floor of
+  // anchored.cpp:24), and its nu and om (the operands of A and g in it)
+  T cap = T(0), rmax = T(0), end_nu = T(0), end_om = T(0);
 
   // one forward step; with rec the lane's column values go to row t - t0 of
   // dst (the global buffer, or this warp's shared sub-segment buffer)
@@ -170,16 +186,22 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     const int j = t - lane;
     T u_in = __shfl_up_sync(FULL, u_bot, 1);
     T s_in = __shfl_up_sync(FULL, rw.s[R - 1], 1);
-    if (lane == 0) { u_in = c0; s_in = c0; }
+    if (lane == 0) { u_in = ANCH ? T(0) : c0; s_in = u_in; }
     if (j == 0) {
 #pragma unroll
       for (int r = 0; r < R; ++r) { rw.mu[r] = T(0); rw.om[r] = T(0); rw.s[r] = T(0); }
       s_top = T(0);
+      if (ANCH) {
+        if (emu == 0) s_top = c0;
+#pragma unroll
+        for (int r = 1; r < R; ++r)
+          if (emu == r) rw.s[r - 1] = c0;
+      }
     }
     const bool act = (unsigned)j <= (unsigned)m;
     const uint32_t hb = (act && j > 0) ? (uint32_t)hap[j - 1] : 0u;
-    T d0, d1, d2;
-    column<T, R, GEN, false>(rw, hb, s_top, u_in, k2, x, u_bot, d0, d1, d2);
+    T tmu = T(0), tnu = T(0), tom = T(0);
+    column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
     s_top = s_in;
     if (rec && act) {
       T* e = dst + (long long)(t - t0) * BFW * kWarp + lane;
@@ -190,7 +212,15 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
       }
       e[2 * R * kWarp] = u_in;
     }
-    if (lane == kWarp - 1 && act) acc += (double)u_bot;
+    if (lane == kWarp - 1 && act) {
+      if (ANCH) {
+        cap = fmaT(gfin, tom, fmaT(A, tnu, tmu));
+        rmax = maxT(rmax, cap);
+        if (j == m) { end_nu = tnu; end_om = tom; }
+      } else {
+        acc += (double)u_bot;
+      }
+    }
   };
   auto save_state = [&](T* __restrict__ area, const int k) {
     T* e = area + (long long)k * CKW * kWarp + lane;
@@ -220,7 +250,8 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     if (!store_all && t % C == 0) save_state(ck, t / C);
     fstep(t, 0, store_all, buf);
   }
-  const double Zs = __shfl_sync(FULL, acc, kWarp - 1);
+  const double Zs = __shfl_sync(FULL, ANCH ? (double)cap : acc, kWarp - 1);
+  const double Zmax = __shfl_sync(FULL, (double)rmax, kWarp - 1);
   double lnN = 0.0;
   for (int i = lane; i < n; i += kWarp) lnN += tb->lnN[rqual[i]];
 #pragma unroll
@@ -260,7 +291,11 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     const bool act = (unsigned)j <= (unsigned)m;
     T in_u = __shfl_down_sync(FULL, top_u, 1);
     T in_s_next = __shfl_down_sync(FULL, top_s, 1);
-    if (lane == kWarp - 1) { in_u = act ? rho : T(0); in_s_next = T(0); }
+    // semiglobal: every (M + I)[n][j] is summed, so u of the bottom row has
+    // adjoint rho; anchored: only the end cell counts (seeded below)
+    if (lane == kWarp - 1) { in_u = (act && !ANCH) ? rho : T(0); in_s_next = T(0); }
+    // anchored end cell at column m: d/dmu = rho, d/dom = rho g, d/dnu = rho A
+    const bool seed = ANCH && lane == kWarp - 1 && j == m;
     const T in_s = pend_s;
     pend_s = in_s_next;
     if (!act) {
@@ -283,8 +318,9 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
 #pragma unroll
     for (int r = R - 1; r >= 0; --r) {
       const T sb = cs, ub = cu;
-      const T omb = fmaT(x, ome[r], k2 * sb);
-      const T mub = ub + sb + ome[r];
+      const bool sd = seed && r == R - 1;
+      const T omb = fmaT(x, ome[r], k2 * sb) + (sd ? rho * gfin : T(0));
+      const T mub = ub + sb + ome[r] + (sd ? rho : T(0));
       pu[r] = fmaT(ub, nu[r], pu[r]);
       ps[r] = fmaT(sb, nu[r], ps[r]);
       const bool match = rw.rb[r] == hb;
@@ -300,7 +336,7 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
       Bk2 = fmaT(sb, omf[r], Bk2);
       Ax = fmaT(ome[r], omf[r], Ax);
       ome[r] = omb;
-      cu = fmaT(rw.X[r], ub, rw.K[r] * sb);
+      cu = fmaT(rw.X[r], ub, rw.K[r] * sb) + (sd ? rho * A : T(0));
       cs = ups[r];
       ups[r] = up_s;
     }
@@ -341,10 +377,10 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   double jg = 0.0, jx = 0.0, jo0 = 0.0, jo1 = 0.0, jo2 = 0.0, jo3 = 0.0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int i = lane * R + r;
-    if (i < n) {
+    const int i = lane * R + r - v;
+    if (i >= 0 && i < n) {
       const unsigned q = rqual[i];
-      const bool last = i == n - 1;
+      const bool last = !ANCH && i == n - 1;
       const double bX = (double)rw.X[r] * (double)pu[r];
       const double bK = (double)rw.K[r] * (double)ps[r];
       jg += (bX * (last ? gs.dlnA_g : gs.dlnX_g) + bK * gs.dlnK_g) * inv + gs.dlnN_g;
@@ -361,6 +397,19 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
   }
   jg += (double)k2 * (double)Bk2 * gs.dlnk2_g * inv;
   jx += ((double)k2 * (double)Bk2 * gs.dlnk2_x + (double)Ax * gs.dx_x) * inv;
+  if (ANCH && lane == kWarp - 1) {
+    // the end cell's own constants: A = (g/4) f_n and g (d ln g / dQg = -ln(10)/10)
+    const double rho_d = ldexp(1.0, rho_log2);
+    const double bA = rho_d * (double)A * (double)end_nu, bg = rho_d * (double)gfin * (double)end_om;
+    const unsigned q = rqual[n - 1];
+    jg += (bA * gs.dlnA_g + bg * gs.dlng_g) * inv;
+    const double d = -bA * gt->dlnN[q] * inv;
+    const int b = gt->bin[q];
+    jo0 += b == 0 ? d : 0.0;
+    jo1 += b == 1 ? d : 0.0;
+    jo2 += b == 2 ? d : 0.0;
+    jo3 += b == 3 ? d : 0.0;
+  }
 #pragma unroll
   for (int s = 16; s; s >>= 1) {
     jg += __shfl_xor_sync(FULL, jg, s);
@@ -371,8 +420,11 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
     jo3 += __shfl_xor_sync(FULL, jo3, s);
   }
   if (lane == 0) {
-    const double lnC0 = (double)sc.ln_c + log((double)(m + 1));
-    gv.out_ln[o] = log(Zs) - lnC0 + lnN;
+    const double lnC0 = (double)sc.ln_c + (ANCH ? 0.0 : log((double)(m + 1)));
+    // anchored.cpp:24 floors the end cell at 1e-300 of the last row's maximum;
+    // the gradient is that of the unfloored value
+    const double Zc = ANCH ? fmax(Zs, 1e-300 * Zmax) : Zs;
+    gv.out_ln[o] = log(Zc) - lnC0 + lnN;
     double* J = gv.out_jac + o * 6;
     J[0] = jg;
     J[1] = jx;
@@ -392,7 +444,7 @@ __device__ __noinline__ void grad_pair(const BatchView& bv, const GradView& gv, 
 template <typename T> struct GradMinBlocks { static constexpr int value = 3; };
 template <> struct GradMinBlocks<double> { static constexpr int value = 1; };
 
-template <typename T>
+template <typename T, bool ANCH>
 __global__ void __launch_bounds__(kWarpsPerBlock * kWarp, GradMinBlocks<T>::value)
 pairhmm_grad_kernel(const BatchView bv, const GradView gv, const Tables<T>* __restrict__ gtab,
                     const Scalars<T> sc, const GradTables* __restrict__ gtt, const GradScalars gs) {
@@ -429,8 +481,8 @@ pairhmm_grad_kernel(const BatchView bv, const GradView gv, const Tables<T>* __re
     const bool gen = code_general(code);
 #define VD_GCASE(r)                                                                          \
   case r:                                                                                    \
-    if (gen) grad_pair<T, r, true>(bv, gv, item, &tab, sc, &gt, gs, lane, slot, sbuf);     \
-    else grad_pair<T, r, false>(bv, gv, item, &tab, sc, &gt, gs, lane, slot, sbuf);        \
+    if (gen) grad_pair<T, r, true, ANCH>(bv, gv, item, &tab, sc, &gt, gs, lane, slot, sbuf); \
+    else grad_pair<T, r, false, ANCH>(bv, gv, item, &tab, sc, &gt, gs, lane, slot, sbuf);    \
     break;
     switch (code_R(code)) {
       VD_GCASE(1) VD_GCASE(2) VD_GCASE(3) VD_GCASE(4) VD_GCASE(5) VD_GCASE(6) VD_GCASE(7) VD_GCASE(8)

@@ -13,7 +13,11 @@ constexpr int dyn_smem() { return kWarpsPerBlock * grad_smem_per_warp<T>(); }
 // the sub-segment buffers exceed the 48 KB default of dynamic shared memory
 template <typename T>
 cudaError_t allow_smem() {
-  return cudaFuncSetAttribute(pairhmm_grad_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem<T>());
+  cudaError_t e = cudaFuncSetAttribute(pairhmm_grad_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       dyn_smem<T>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(pairhmm_grad_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              dyn_smem<T>());
 }
 }  // namespace
 
@@ -22,7 +26,12 @@ cudaError_t launch_grad_f32(const BatchView& bv, const GradView& gv, const Table
                             cudaStream_t stream) {
   cudaError_t e = allow_smem<float>();
   if (e != cudaSuccess) return e;
-  pairhmm_grad_kernel<float><<<grid, kWarpsPerBlock * kWarp, dyn_smem<float>(), stream>>>(bv, gv, tab, sc, gt, gs);
+  if (gv.anchored)
+    pairhmm_grad_kernel<float, true><<<grid, kWarpsPerBlock * kWarp, dyn_smem<float>(), stream>>>(bv, gv, tab, sc, gt,
+                                                                                                  gs);
+  else
+    pairhmm_grad_kernel<float, false><<<grid, kWarpsPerBlock * kWarp, dyn_smem<float>(), stream>>>(bv, gv, tab, sc,
+                                                                                                   gt, gs);
   return cudaGetLastError();
 }
 
@@ -31,17 +40,21 @@ cudaError_t launch_grad_f64(const BatchView& bv, const GradView& gv, const Table
                             cudaStream_t stream) {
   cudaError_t e = allow_smem<double>();
   if (e != cudaSuccess) return e;
-  pairhmm_grad_kernel<double><<<grid, kWarpsPerBlock * kWarp, dyn_smem<double>(), stream>>>(bv, gv, tab, sc, gt,
-                                                                                             gs);
+  if (gv.anchored)
+    pairhmm_grad_kernel<double, true><<<grid, kWarpsPerBlock * kWarp, dyn_smem<double>(), stream>>>(bv, gv, tab, sc,
+                                                                                                    gt, gs);
+  else
+    pairhmm_grad_kernel<double, false><<<grid, kWarpsPerBlock * kWarp, dyn_smem<double>(), stream>>>(bv, gv, tab, sc,
+                                                                                                     gt, gs);
   return cudaGetLastError();
 }
 
 cudaError_t occupancy_grad(bool fp64, int* blocks_per_sm) {
   cudaError_t e = fp64 ? allow_smem<double>() : allow_smem<float>();
   if (e != cudaSuccess) return e;
-  return fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_grad_kernel<double>,
+  return fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_grad_kernel<double, false>,
                                                               kWarpsPerBlock * kWarp, dyn_smem<double>())
-              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_grad_kernel<float>,
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_grad_kernel<float, false>,
                                                               kWarpsPerBlock * kWarp, dyn_smem<float>());
 }
 

@@ -711,6 +711,7 @@ void build_grad_tables(double g, double x, const double* offsets, GradTables* gt
   gs->dlnX_g = (2.0 / a) * dg;
   gs->dlnA_g = (1.0 / g + 2.0 / a) * dg;
   gs->dlnk2_g = (1.0 / g + 2.0 / a) * dg;
+  gs->dlng_g = (1.0 / g) * dg;
   gs->dlnK_x = (-1.0 / (1.0 - x)) * dx;
   gs->dlnX_x = (1.0 / x) * dx;
   gs->dlnk2_x = (-1.0 / (1.0 - x)) * dx;
@@ -1401,15 +1402,14 @@ int vd_forward_backward(vd_engine* e, const vd_batch* b, const vd_params* p, int
   int rc = validate_params(p);
   if (!rc) rc = validate_batch(b);
   if (rc) return rc;
-  if (p->anchored) return fail(VD_EINVAL, "the gradient covers the semiglobal model (anchored = 0)");
   if (p->schedule != VD_SCHEDULE_BATCHED) return fail(VD_EINVAL, "the gradient runs the batched schedule only");
   if (!(p->gap > 0.0) || !(p->ext > 0.0)) return fail(VD_EINVAL, "the gradient needs gap > 0 and ext > 0");
   if (checkpoint != VD_CHECKPOINT_SQRT && checkpoint != VD_CHECKPOINT_ALL) return fail(VD_EINVAL, "unknown checkpoint mode");
   const int64_t n_out = batch_outputs(b);
   if (n_out > 0 && (!out_ln || !out_jac)) return fail(VD_EINVAL, "out_ln or out_jac is NULL");
   for (int64_t r = 0; r < b->n_reads; ++r)
-    if (b->read_off[r + 1] - b->read_off[r] > kStripRows)
-      return fail(VD_EINVAL, "the gradient supports reads of at most 256 bases");
+    if (b->read_off[r + 1] - b->read_off[r] + (p->anchored ? 1 : 0) > kStripRows)
+      return fail(VD_EINVAL, "the gradient supports reads of at most 256 bases (255 anchored)");
   std::lock_guard<std::mutex> lk(e->mu);
   DeviceGuard guard(e->device);
   vd_grad_stats s{};
@@ -1422,7 +1422,7 @@ int vd_forward_backward(vd_engine* e, const vd_batch* b, const vd_params* p, int
   // every input on the device once; reads carry the code of the forward tiers
   HostChunk c;
   c.ra = 0; c.rb = b->n_reads; c.ha = 0; c.hb = b->n_haps;
-  finish_chunk_common(c, b, e->htab, offsets, false);
+  finish_chunk_common(c, b, e->htab, offsets, p->anchored != 0);
   std::vector<RescueEntry> items;
   items.reserve((size_t)n_out);
   std::vector<int64_t> empty_slots;
@@ -1493,6 +1493,7 @@ int vd_forward_backward(vd_engine* e, const vd_batch* b, const vd_params* p, int
   gv.scratch = d + o_scratch;
   gv.slot_bytes = slot_bytes;
   gv.store_all = store_all ? 1 : 0;
+  gv.anchored = p->anchored ? 1 : 0;
   gv.error_flag = (int*)(cnt + 4);
   const TableSet* dt = (const TableSet*)e->dtab.p;
   const TableSet* ht = e->htab;
