@@ -553,8 +553,8 @@ def main():
             "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak.value, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / peak.value, 4), "traffic": traffic,
                          "flops_per_cell": FLOPS_PER_CELL,
-                         "kernel": "pairhmm_kernel<float> (primary tier)" if args.workload == "config1"
-                         else "all three tiers (whole step)",
+                         "kernel": "FP32 tier: pairhmm_pair_kernel x2 + pairhmm_kernel<float>"
+                         if args.workload == "config1" else "all three tiers (whole step)",
                          "primary_ms": round(primary_ms, 3),
                          "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
                          "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},
