@@ -142,7 +142,8 @@ def _anchored_windows(seed, sites=12, reads=10):
             np.concatenate([ref[:p], S.ALPHABET[rng.integers(0, 4, k)], ref[p:]])
         for _ in range(reads):
             src = alt if rng.random() < 0.5 else ref
-            a, b = int(rng.integers(10, 80)), int(rng.integers(p + 20, p + 110))
+            a = int(rng.integers(10, 80))
+            b = int(rng.integers(p + 20, min(p + 110, a + 250)))
             read = src[a:b].copy()
             flip = rng.random(len(read)) < 0.02
             read[flip] = S.ALPHABET[(np.searchsorted(S.ALPHABET, read[flip]) + 1) % 4]
