@@ -104,6 +104,8 @@ typedef struct vd_stats {
   int64_t live_bytes;       /* device bytes held by the call's buffers */
   double primary_ms;        /* device time of the primary (FP32, or FP64) tier alone */
   double rescue_ms;         /* device time of the two FP64 rescue tiers */
+  int64_t shared_cells;     /* of dp_cells, those of haplotype columns that repeat the previous
+                               haplotype of the region and were not streamed again */
 } vd_stats;
 
 typedef struct vd_engine vd_engine;

@@ -394,3 +394,58 @@ def test_region_shards_score_like_the_whole_batch():
         full[pos] = eng.forward(sub, params)[0]
     np.testing.assert_array_equal(full, whole)
     eng.close()
+
+
+def _prefix_regions(seed):
+    """Regions whose haplotypes repeat the previous one's first bases in every pattern the
+    two-read kernel distinguishes: a snapshot taken while the previous haplotype streams, one
+    kept from the previous haplotype's own start, none (a shorter shared prefix), identical
+    haplotypes, a haplotype that is a prefix of the previous one or extends it, a share that
+    leaves one column to stream, prefixes below the 32-column minimum, an empty haplotype."""
+    rng = np.random.default_rng(seed)
+    qf = S._q_standard(rng)
+
+    def snv(h, p):
+        h = h.copy()
+        h[p] = S.ALPHABET[S.ALPHABET != h[p]][rng.integers(0, 3)]
+        return h
+
+    base = S._random_hap(rng, 400)
+    chain = [base] + [snv(base, p) for p in (300, 100, 250, 250, 60, 380, 40, 40, 40, 200)]
+    b2 = S._random_hap(rng, 300)
+    nested = [b2, b2[:200], b2.copy(), b2.copy(), np.concatenate([b2, S._random_hap(rng, 50)])]
+    b3 = S._random_hap(rng, 33)
+    short = [b3, b3.copy(), snv(S._random_hap(rng, 40), 5), S._random_hap(rng, 20), S._random_hap(rng, 20)]
+    b4 = S._random_hap(rng, 250)
+    gapped = [b4, np.empty(0, np.uint8), b4.copy(), snv(b4, 120)]
+    regions = []
+    for haps in (chain, nested, short, gapped, [base]):
+        src = [h for h in haps if len(h) > 0]
+        nr = int(rng.integers(9, 15))
+        lengths = np.repeat(rng.integers(20, 257, nr), 2)[:nr]  # pairs of reads with the same rows per lane
+        lengths[0] = 300  # one read longer than a strip (its own items, no sharing)
+        reads, quals = S._sim_reads(rng, src, nr, lengths, 0.01, 0.001, qf)
+        regions.append((haps, reads, quals))
+    return S._assemble("prefixes", regions, S.GAP_Q45, S.EXT_Q10, {"seed": seed})
+
+
+@pytest.mark.parametrize("max_item_columns", [0, 450])
+def test_shared_haplotype_prefixes(max_item_columns):
+    """Two-read items start a haplotype past the prefix it shares with the previous haplotype
+    of its region; the skipped columns are bit-identical to streaming them (the plain
+    schedule shares nothing) and the scores match the FP64 oracle."""
+    w = _prefix_regions(77)
+    eng = native.Engine(0, 4096)
+    eng.set_tuning(max_item_columns=max_item_columns)
+    batched, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    plain, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED, schedule=native.VD_SCHEDULE_PLAIN)
+    a, st_a = eng.forward(_packed(w), batched)
+    b, st_b = eng.forward(_packed(w), plain)
+    assert 0 < st_a.shared_cells < st_a.dp_cells and st_b.shared_cells == 0
+    np.testing.assert_array_equal(a, b)
+    assert_mixed_close(a, _oracle_workload(w))
+    plan = eng.plan(_packed(w), batched)
+    assert plan.run().shared_cells == st_a.shared_cells
+    np.testing.assert_array_equal(plan.fetch(), a)
+    plan.close()
+    eng.close()

@@ -100,6 +100,8 @@ struct BatchView {
   const int32_t* hap_sel;     // nullable: indirect haplotype lists
   const int64_t* out_sel;     // nullable: indirect output slots
   double* out;
+  const int32_t* hap_share;   // nullable: per haplotype, Q >= 0 when it shares DP columns 0..Q
+                              // with the previous haplotype of its region (two-read items)
 };
 
 struct QueueView {

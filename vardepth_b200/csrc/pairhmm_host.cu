@@ -320,9 +320,11 @@ struct HostChunk {
   std::vector<int32_t> hap_sel;    // pair form
   std::vector<int64_t> out_sel;    // pair form (chunk-local output slots)
   std::vector<int64_t> out_global; // pair form: batch output index of each local slot
+  std::vector<int32_t> hap_share;  // region form, two-read items: shared prefix column per haplotype
   int64_t out_begin = 0;           // region form: first batch output slot
   int64_t n_out = 0;
   int64_t cells = 0;
+  int64_t shared_cells = 0;        // of cells, those two-read items skip by prefix sharing
   int64_t pairs_scored = 0;
   int max_hap = 0;
   bool any_long = false;           // a read longer than 32 (the robust tier strip-mines it)
@@ -443,6 +445,39 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
   for (int64_t h = c.ha; h < c.hb; ++h) c.max_hap = std::max<int>(c.max_hap, (int)(b->hap_off[h + 1] - b->hap_off[h]));
 }
 
+// Shared haplotype prefixes of one region (two-read items).  share[h] = Q >= 0
+// says that haplotype h agrees with haplotype h-1 on its first Q bases, so DP
+// columns 0..Q of the two are the same and the two-read kernel starts h at
+// column Q+1 from the lane states it laid down at column Q of h-1.  Each warp
+// holds one such snapshot, so Q is used when the snapshot can be taken while
+// h-1 streams (Q at or past the column h-1 itself started from) or when it
+// is still there (Q equal to the share of h-1); otherwise -1.  Q stays below
+// the length of h (h streams at least one column) and at or above
+// kMinShareColumns: a snapshot puts 32 steps of the ramp loop into the
+// haplotype that takes it.
+constexpr int kMinShareColumns = 32;
+
+void region_shares(const vd_batch* b, int64_t h_lo, int64_t h_hi, int32_t* share) {
+  int prev_q = -1;
+  for (int64_t h = h_lo; h < h_hi; ++h) {
+    int q = -1;
+    if (h > h_lo) {
+      const int64_t a0 = b->hap_off[h - 1], b0 = b->hap_off[h];
+      const int ma = (int)(b0 - a0), mb = (int)(b->hap_off[h + 1] - b0);
+      if (ma > 0 && mb > 0) {
+        const int lim = std::min(ma, mb - 1);
+        int l = 0;
+        while (l < lim && b->hap_bases[a0 + l] == b->hap_bases[b0 + l]) ++l;
+        if (l >= prev_q + 1) q = l;
+        else if (prev_q >= 0 && l >= prev_q) q = prev_q;
+        if (q < kMinShareColumns) q = -1;
+      }
+    }
+    share[h - h_lo] = q;
+    prev_q = q;
+  }
+}
+
 // Work items of a region chunk: one item per read with the region's non-empty
 // haplotypes as contiguous runs; reads longer than a strip get one item per
 // haplotype (their strip boundary scratch holds one haplotype).  With
@@ -475,10 +510,13 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   struct Slice {
     std::vector<WorkItem> items;
     std::vector<int64_t> cost;
-    int64_t cells = 0, pairs = 0;
+    int64_t cells = 0, shared = 0, pairs = 0;
   };
   const int64_t nslices = std::max<int64_t>(1, std::min<int64_t>(256, ng / 16));
   std::vector<Slice> slices((size_t)nslices);
+  const bool sharing = pair_reads && !anchored && !plain;
+  c.hap_share.clear();
+  if (sharing) c.hap_share.assign((size_t)(c.hb - c.ha), -1);
   parallel_for(nslices, 1, [&](int64_t s_lo, int64_t s_hi) {
    for (int64_t si = s_lo; si < s_hi; ++si) {
     Slice& sl = slices[(size_t)si];
@@ -489,6 +527,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
     const int64_t h_lo = b->region_hap_off[g], h_hi = b->region_hap_off[g + 1];
     const int64_t nh = h_hi - h_lo;
     const int64_t region_out = region_out_of[g - g0];
+    if (sharing) region_shares(b, h_lo, h_hi, c.hap_share.data() + (h_lo - c.ha));
     // emit the haplotype runs of read r (and r2 >= 0 riding along)
     auto emit = [&](int64_t r, int64_t r2) {
       const int32_t code = c.read_code[r - c.ra];
@@ -507,9 +546,13 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
         while (run_end < h_hi) {
           const int m = (int)(b->hap_off[run_end + 1] - b->hap_off[run_end]);
           if (m <= 0) break;
-          if (run_end > h && (plain || multistrip || stream + m + 1 > kMaxStream)) break;
-          stream += m + 1;
+          // a haplotype after the first of a two-read run streams only the
+          // columns past its shared prefix
+          const int col0 = (r2 >= 0 && run_end > h && sharing) ? c.hap_share[run_end - c.ha] + 1 : 0;
+          if (run_end > h && (plain || multistrip || stream + m + 1 - col0 > kMaxStream)) break;
+          stream += m + 1 - col0;
           sl.cells += (int64_t)(n + n2) * m;
+          if (col0 > 0) sl.shared += (int64_t)(n + n2) * (col0 - 1);
           sl.pairs += r2 >= 0 ? 2 : 1;
           ++run_end;
         }
@@ -557,6 +600,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
     c.items.insert(c.items.end(), sl.items.begin(), sl.items.end());
     cost.insert(cost.end(), sl.cost.begin(), sl.cost.end());
     c.cells += sl.cells;
+    c.shared_cells += sl.shared;
     c.pairs_scored += sl.pairs;
   }
   const int64_t out = region_out_of[ng];
@@ -645,8 +689,8 @@ void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64
 
 // Device bytes a chunk needs (inputs, lists, outputs, rescue lists, scratch).
 struct Layout {
-  size_t o_rb, o_rq, o_roff, o_rcode, o_hb, o_hoff, o_hsel, o_osel, o_items, o_out, o_sp1, o_sp2, o_cnt,
-      o_scratch, total;
+  size_t o_rb, o_rq, o_roff, o_rcode, o_hb, o_hoff, o_hsel, o_osel, o_hshare, o_items, o_out, o_sp1, o_sp2,
+      o_cnt, o_scratch, total;
   int64_t scratch_stride;  // double2 records per warp slot
   int64_t warps;
 };
@@ -665,6 +709,7 @@ Layout layout_for(const HostChunk& c, const vd_batch* b, int64_t warps) {
   L.o_hoff = take(c.hap_off.size() * sizeof(int64_t));
   L.o_hsel = take(c.hap_sel.size() * sizeof(int32_t));
   L.o_osel = take(c.out_sel.size() * sizeof(int64_t));
+  L.o_hshare = take(c.hap_share.size() * sizeof(int32_t));
   L.o_items = take(c.items.size() * sizeof(WorkItem));
   L.o_out = take((size_t)c.n_out * sizeof(double));
   L.o_sp1 = take((size_t)std::max<int64_t>(1, c.pairs_scored) * sizeof(RescueEntry));
@@ -757,6 +802,7 @@ BatchView batch_view(vd_plan* pl) {
   bv.hap_off = (const int64_t*)(d + pl->L.o_hoff);
   bv.hap_sel = pl->chunk.hap_sel.empty() && pl->chunk.out_sel.empty() ? nullptr : (const int32_t*)(d + pl->L.o_hsel);
   bv.out_sel = bv.hap_sel ? (const int64_t*)(d + pl->L.o_osel) : nullptr;
+  bv.hap_share = pl->chunk.hap_share.empty() ? nullptr : (const int32_t*)(d + pl->L.o_hshare);
   bv.out = (double*)(d + pl->L.o_out);
   return bv;
 }
@@ -783,6 +829,7 @@ int upload_chunk(vd_plan* pl, const vd_batch* b, int64_t* h2d) {
   if ((rc = put(pl->L.o_hoff, c.hap_off.data(), c.hap_off.size() * sizeof(int64_t)))) return rc;
   if ((rc = put(pl->L.o_hsel, c.hap_sel.data(), c.hap_sel.size() * sizeof(int32_t)))) return rc;
   if ((rc = put(pl->L.o_osel, c.out_sel.data(), c.out_sel.size() * sizeof(int64_t)))) return rc;
+  if ((rc = put(pl->L.o_hshare, c.hap_share.data(), c.hap_share.size() * sizeof(int32_t)))) return rc;
   if ((rc = put(pl->L.o_items, c.items.data(), c.items.size() * sizeof(WorkItem)))) return rc;
   if (c.n_out > 0) {
     fill_kernel<<<(int)std::min<int64_t>(4096, (c.n_out + 255) / 256), 256, 0, pl->stream>>>(
@@ -1249,6 +1296,7 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     if ((rc = enqueue_counter_read(&pl, sl.hcnt))) return rc;
     sl.busy = true;
     s.dp_cells += c.cells;
+    s.shared_cells += c.shared_cells;
     s.work_items += (int64_t)c.items.size();
     ++s.batches;
     ++chunk_index;
@@ -1341,6 +1389,7 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
     vd_stats s{};
     s.pairs = pl->chunk.n_out;
     s.dp_cells = pl->chunk.cells;
+    s.shared_cells = pl->chunk.shared_cells;
     s.work_items = (int64_t)pl->chunk.items.size();
     s.batches = 1;
     s.rescued_fp64 = r1;

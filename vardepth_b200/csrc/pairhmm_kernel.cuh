@@ -298,7 +298,9 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       s_top = s_in;
       if (last) {
         accumulate(tmu, tnu, tom);
-        if (!ANCH) { acc64 += (double)acc32; acc32 = T(0); }
+        // lane 31 moves its row sum into FP64 after its columns 8r+7 (by
+        // column, as the two-read path does, so both give the same bits)
+        if (!ANCH && lane == kWarp - 1 && ((p - S_cur) & 7) == 7) { acc64 += (double)acc32; acc32 = T(0); }
       } else {
         if (lane == kWarp - 1 && active) {
           scratch[p] = T2{rw.s[R - 1], u_bot};
@@ -346,7 +348,15 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       const int gen_end = (k < K) ? min(S + kWarp, Snext) : S + kWarp;
       for (; t < gen_end; ++t) gstep(t);
       if (k < K) {
-        // all lanes are inside haplotype k for t in [S + 32, Snext)
+        // all lanes are inside haplotype k for t in [S + 32, Snext).  Lane
+        // 31's column at step t is t - 31 - S; single steps bring it to a
+        // multiple of 8, so every block of 8 ends on a column 8r+7
+        const int lead = -(kWarp - 1) - S;
+        for (; t < Snext && ((lead + t) & 7) != 0; ++t) {
+          sstep((uint32_t)hp[t - lane], t - lane, t);
+          if (last && !ANCH && ((lead + t) & 7) == 7) { acc64 += (double)acc32; acc32 = T(0); }
+        }
+        static_assert(kUnroll == 8, "blocks of 8 steps flush once, at their last column");
         for (; t + kUnroll <= Snext; t += kUnroll) {
           const uint8_t* q = hp + (t - lane);
 #pragma unroll
@@ -354,10 +364,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
           if (last && !ANCH) { acc64 += (double)acc32; acc32 = T(0); }
           if (!last) __syncwarp();
         }
-        for (; t < Snext; ++t) {
-          sstep((uint32_t)hp[t - lane], t - lane, t);
-          if (last && !ANCH) { acc64 += (double)acc32; acc32 = T(0); }
-        }
+        for (; t < Snext; ++t) sstep((uint32_t)hp[t - lane], t - lane, t);  // columns 8r..8r+6: no flush
       }
       S = Snext;
     }
@@ -455,7 +462,7 @@ __device__ __forceinline__ float2 shfl_up2(float2 v) {
 template <int R>
 __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv, const ItemRef it,
                                           const Tables<float>* __restrict__ tb, const Scalars<float> sc,
-                                          const int lane) {
+                                          const int lane, float2* __restrict__ sv) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr double kLn2 = 0.6931471805599453094;
   const WorkItem& w = it.w;
@@ -516,10 +523,24 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
     rw.s[r] = make_float2(0.f, 0.f);
   }
 
-  int kL = -1, next_reset = 0, S_cur = -1;
+  // Shared haplotype prefixes: when hap_share[h] = Q >= 0, haplotype h agrees
+  // with haplotype h-1 of the same region on its first Q bases, so DP columns
+  // 0..Q are the same for both.  The lanes lay their state down in shared
+  // memory (sv) when they finish column Q of h-1 and start h at column Q+1
+  // from it, so the stream carries only columns Q+1..m of h.  Lane 31 also
+  // carries its row sum across.  The row sums are flushed from FP32 into FP64
+  // after every column 8r+7 of lane 31 (by column, not by step), so a shared
+  // and an unshared pass give the same bits.
+  auto share_of = [&](int k) -> int {
+    return (k > 0 && k < K && bv.hap_share != nullptr) ? (int)bv.hap_share[w.hap_begin + k] : -1;
+  };
+  int kL = -1, next_reset = 0, S_cur = -1, c0 = 0, save_at = -1;
   const uint8_t* hp = bv.hap_bases;
   float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
   double accA = 0.0, accB = 0.0;
+  // snapshot layout, slot-major with one entry per lane: mu, om, s of every
+  // row, s_top, the FP32 row sums, then the two FP64 row sums
+  double* const svd = reinterpret_cast<double*>(sv + (3 * R + 2) * kWarp);
 
   auto finalize = [&](int k) {
     const int64_t h = w.hap_begin + k;
@@ -546,7 +567,32 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
     accB += (double)acc32.y;
     acc32 = make_float2(0.f, 0.f);
   };
+  auto save = [&]() {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      sv[(3 * r) * kWarp + lane] = rw.mu[r];
+      sv[(3 * r + 1) * kWarp + lane] = rw.om[r];
+      sv[(3 * r + 2) * kWarp + lane] = rw.s[r];
+    }
+    sv[3 * R * kWarp + lane] = s_top;
+    sv[(3 * R + 1) * kWarp + lane] = acc32;
+    svd[lane] = accA;
+    svd[kWarp + lane] = accB;
+  };
+  auto restore = [&]() {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      rw.mu[r] = sv[(3 * r) * kWarp + lane];
+      rw.om[r] = sv[(3 * r + 1) * kWarp + lane];
+      rw.s[r] = sv[(3 * r + 2) * kWarp + lane];
+    }
+    s_top = sv[3 * R * kWarp + lane];
+    acc32 = sv[(3 * R + 1) * kWarp + lane];
+    accA = svd[lane];
+    accB = svd[kWarp + lane];
+  };
 
+  // step with per-lane haplotype bookkeeping (ramps, snapshots, short haplotypes)
   auto gstep = [&](int t) {
     const int p = t - lane;
     float2 u_in = shfl_up2(u_bot);
@@ -554,35 +600,49 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
     if (p == next_reset) {
       if (kL >= 0 && lane == kWarp - 1) finalize(kL);
       ++kL;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        rw.mu[r] = make_float2(0.f, 0.f);
-        rw.om[r] = make_float2(0.f, 0.f);
-        rw.s[r] = make_float2(0.f, 0.f);
-      }
-      s_top = make_float2(0.f, 0.f);
-      acc32 = make_float2(0.f, 0.f);
-      accA = accB = 0.0;
       S_cur = p;
+      save_at = -1;
       if (kL < K) {
+        const int q = share_of(kL);
+        c0 = q + 1;
+        if (q >= 0) {
+          restore();
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            rw.mu[r] = make_float2(0.f, 0.f);
+            rw.om[r] = make_float2(0.f, 0.f);
+            rw.s[r] = make_float2(0.f, 0.f);
+          }
+          s_top = make_float2(0.f, 0.f);
+          acc32 = make_float2(0.f, 0.f);
+          accA = accB = 0.0;
+        }
         const int64_t h = w.hap_begin + kL;
         const int64_t ho = bv.hap_off[h];
-        hp = bv.hap_bases + ho - 1 - p;
-        next_reset = p + (int)(bv.hap_off[h + 1] - ho) + 1;
+        hp = bv.hap_bases + ho + c0 - 1 - p;
+        next_reset = p + (int)(bv.hap_off[h + 1] - ho) + 1 - c0;
+        // the next haplotype starts from column qn: a snapshot of it is taken
+        // here, or (qn == c0 - 1) the one this haplotype started from stays
+        const int qn = share_of(kL + 1);
+        if (qn >= c0) save_at = p + (qn - c0);
       } else {
         next_reset = INT_MAX;
       }
     }
     const bool active = kL >= 0 && kL < K;
-    const uint32_t hb = (active && p != S_cur) ? (uint32_t)hp[p] : 0u;
+    const uint32_t hb = (active && !(p == S_cur && c0 == 0)) ? (uint32_t)hp[p] : 0u;
     u_in = lane0 ? c2 : u_in;
     s_in = lane0 ? c2 : s_in;
     column2<R>(rw, hb, s_top, u_in, k2, x, u_bot);
     s_top = s_in;
     acc32 = __fadd2_rn(acc32, u_bot);
-    flush();
+    // lane 31 alone flushes, after its columns 8r+7
+    if (lane == kWarp - 1 && ((c0 + p - S_cur) & 7) == 7) flush();
+    if (p == save_at) save();
   };
 
+  // step with every lane inside the same haplotype past its start column
   auto sstep = [&](uint32_t hb) {
     float2 u_in = shfl_up2(u_bot);
     float2 s_in = shfl_up2(rw.s[R - 1]);
@@ -595,21 +655,42 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
 
   int t = 0, S = 0;
   for (int k = 0; k <= K; ++k) {
-    int mk = 0;
-    if (k < K) mk = (int)(bv.hap_off[w.hap_begin + k + 1] - bv.hap_off[w.hap_begin + k]);
-    const int Snext = S + mk + 1;
+    int seg = 0, ck = 0, w0 = -1;
+    if (k < K) {
+      const int mk = (int)(bv.hap_off[w.hap_begin + k + 1] - bv.hap_off[w.hap_begin + k]);
+      ck = share_of(k) + 1;
+      seg = mk + 1 - ck;
+      const int qn = share_of(k + 1);
+      if (qn >= ck) w0 = S + (qn - ck);  // lanes take the snapshot at steps w0 .. w0 + 31
+    }
+    const int Snext = S + seg;
     const int gen_end = (k < K) ? min(S + kWarp, Snext) : S + kWarp;
     for (; t < gen_end; ++t) gstep(t);
     if (k < K) {
-      for (; t + kUnroll <= Snext; t += kUnroll) {
-        const uint8_t* q = hp + (t - lane);
+      // all lanes are inside haplotype k for t in [S + 32, Snext); the
+      // snapshot window of the next haplotype runs through gstep
+      while (t < Snext) {
+        if (w0 >= 0 && t >= w0 && t < w0 + kWarp) {
+          gstep(t);
+          ++t;
+          continue;
+        }
+        const int stop = (w0 >= 0 && t < w0) ? min(w0, Snext) : Snext;
+        // lane 31's column at step t is ck + (t - 31 - S); single steps bring
+        // it to a multiple of 8, so every block of 8 ends on a column 8r+7
+        const int lead = ck - (kWarp - 1) - S;
+        for (; t < stop && ((lead + t) & 7) != 0; ++t) {
+          sstep((uint32_t)hp[t - lane]);
+          if (((lead + t) & 7) == 7) flush();
+        }
+        static_assert(kUnroll == 8, "blocks of 8 steps flush once, at their last column");
+        for (; t + kUnroll <= stop; t += kUnroll) {
+          const uint8_t* q = hp + (t - lane);
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) sstep((uint32_t)q[u]);
-        flush();
-      }
-      for (; t < Snext; ++t) {
-        sstep((uint32_t)hp[t - lane]);
-        flush();
+          for (int u = 0; u < kUnroll; ++u) sstep((uint32_t)q[u]);
+          flush();
+        }
+        for (; t < stop; ++t) sstep((uint32_t)hp[t - lane]);  // columns 8r..8r+6: no flush
       }
     }
     S = Snext;
@@ -717,6 +798,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
 pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
                     const Scalars<float> sc) {
   __shared__ Tables<float> tab;
+  // per warp: the lane states laid down at a shared haplotype prefix
+  __shared__ float2 saves[kWarpsPerBlock][(3 * kHiR + 4) * kWarp];
   {
     const int words = (int)(sizeof(Tables<float>) / sizeof(int));
     const int* src = reinterpret_cast<const int*>(gtab);
@@ -725,6 +808,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
   }
   __syncthreads();
   const int lane = threadIdx.x & (kWarp - 1);
+  float2* sv = saves[threadIdx.x >> 5];
   for (;;) {
     unsigned long long i = 0;
     if (lane == 0) i = atomicAdd(qv.head, 1ull);
@@ -736,7 +820,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
     it.tier = 0;
     switch (code_R(it.w.code)) {
 #define VD_PCASE(r) \
-      case r: if constexpr (r >= kLoR && r <= kHiR) process_pair<r>(bv, qv, it, &tab, sc, lane); break;
+      case r: if constexpr (r >= kLoR && r <= kHiR) process_pair<r>(bv, qv, it, &tab, sc, lane, sv); break;
       VD_PCASE(1) VD_PCASE(2) VD_PCASE(3) VD_PCASE(4) VD_PCASE(5) VD_PCASE(6) VD_PCASE(7) VD_PCASE(8)
 #undef VD_PCASE
       default: break;
