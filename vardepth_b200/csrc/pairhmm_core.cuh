@@ -100,8 +100,11 @@ struct BatchView {
   const int32_t* hap_sel;     // nullable: indirect haplotype lists
   const int64_t* out_sel;     // nullable: indirect output slots
   double* out;
-  const int32_t* hap_share;   // nullable: per haplotype, Q >= 0 when it shares DP columns 0..Q
-                              // with the previous haplotype of its region (two-read items)
+  const int32_t* hap_order;   // nullable: two-read items read their haplotypes through it (a
+                              // region's haplotypes in lexicographic order; the entry is the
+                              // chunk-local haplotype and, added to out_begin, the output slot)
+  const int32_t* hap_share;   // nullable, same positions: Q >= 0 when the haplotype shares DP
+                              // columns 0..Q with the one before it
 };
 
 struct QueueView {

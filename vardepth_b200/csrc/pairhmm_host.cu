@@ -320,7 +320,9 @@ struct HostChunk {
   std::vector<int32_t> hap_sel;    // pair form
   std::vector<int64_t> out_sel;    // pair form (chunk-local output slots)
   std::vector<int64_t> out_global; // pair form: batch output index of each local slot
-  std::vector<int32_t> hap_share;  // region form, two-read items: shared prefix column per haplotype
+  std::vector<int32_t> hap_order;  // region form, two-read items: chunk-local haplotype at each position
+                                   // (every region's haplotypes in lexicographic order)
+  std::vector<int32_t> hap_share;  // the same positions: shared prefix column with the previous one
   int64_t out_begin = 0;           // region form: first batch output slot
   int64_t n_out = 0;
   int64_t cells = 0;
@@ -445,35 +447,52 @@ void finish_chunk_common(HostChunk& c, const vd_batch* b, const TableSet* ts, bo
   for (int64_t h = c.ha; h < c.hb; ++h) c.max_hap = std::max<int>(c.max_hap, (int)(b->hap_off[h + 1] - b->hap_off[h]));
 }
 
-// Shared haplotype prefixes of one region (two-read items).  share[h] = Q >= 0
-// says that haplotype h agrees with haplotype h-1 on its first Q bases, so DP
-// columns 0..Q of the two are the same and the two-read kernel starts h at
-// column Q+1 from the lane states it laid down at column Q of h-1.  Each warp
-// holds one such snapshot, so Q is used when the snapshot can be taken while
-// h-1 streams (Q at or past the column h-1 itself started from) or when it
-// is still there (Q equal to the share of h-1); otherwise -1.  Q stays below
-// the length of h (h streams at least one column) and at or above
+// Shared haplotype prefixes of one region (two-read items).  The two-read
+// items visit a region's haplotypes in lexicographic order (order[i], i over
+// the region's positions), the depth-first order of their prefix tree, so each
+// haplotype follows the one it shares most with.  share[i] = Q >= 0 says that
+// the haplotype at position i agrees with the one at i-1 on its first Q
+// bases, so DP columns 0..Q of the two are the same and the two-read kernel
+// starts it at column Q+1 from the lane states it laid down at column Q of
+// the previous one.  Each warp holds one such snapshot, so Q is used when the
+// snapshot can be taken while the previous haplotype streams (Q at or past
+// the column that one itself started from) or when it is still there (Q
+// equal to the previous share); otherwise -1.  Q stays below the length of
+// the haplotype (it streams at least one column) and at or above
 // kMinShareColumns: a snapshot puts 32 steps of the ramp loop into the
 // haplotype that takes it.
 constexpr int kMinShareColumns = 32;
 
-void region_shares(const vd_batch* b, int64_t h_lo, int64_t h_hi, int32_t* share) {
+void region_order_and_shares(const vd_batch* b, int64_t h_lo, int64_t h_hi, int64_t ha, int32_t* order,
+                             int32_t* share) {
+  const int64_t nh = h_hi - h_lo;
+  for (int64_t i = 0; i < nh; ++i) order[i] = (int32_t)(h_lo - ha + i);
+  auto bytes = [&](int32_t lh) {
+    const int64_t h = ha + lh;
+    return std::make_pair(b->hap_bases + b->hap_off[h], (size_t)(b->hap_off[h + 1] - b->hap_off[h]));
+  };
+  std::stable_sort(order, order + nh, [&](int32_t x, int32_t y) {
+    const auto [px, nx] = bytes(x);
+    const auto [py, ny] = bytes(y);
+    const int c = nx && ny ? std::memcmp(px, py, std::min(nx, ny)) : 0;
+    return c != 0 ? c < 0 : nx < ny;
+  });
   int prev_q = -1;
-  for (int64_t h = h_lo; h < h_hi; ++h) {
+  for (int64_t i = 0; i < nh; ++i) {
     int q = -1;
-    if (h > h_lo) {
-      const int64_t a0 = b->hap_off[h - 1], b0 = b->hap_off[h];
-      const int ma = (int)(b0 - a0), mb = (int)(b->hap_off[h + 1] - b0);
+    if (i > 0) {
+      const auto [pa, ma] = bytes(order[i - 1]);
+      const auto [pb, mb] = bytes(order[i]);
       if (ma > 0 && mb > 0) {
-        const int lim = std::min(ma, mb - 1);
+        const int lim = (int)std::min(ma, mb - 1);
         int l = 0;
-        while (l < lim && b->hap_bases[a0 + l] == b->hap_bases[b0 + l]) ++l;
+        while (l < lim && pa[l] == pb[l]) ++l;
         if (l >= prev_q + 1) q = l;
         else if (prev_q >= 0 && l >= prev_q) q = prev_q;
         if (q < kMinShareColumns) q = -1;
       }
     }
-    share[h - h_lo] = q;
+    share[i] = q;
     prev_q = q;
   }
 }
@@ -516,7 +535,11 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   std::vector<Slice> slices((size_t)nslices);
   const bool sharing = pair_reads && !anchored && !plain;
   c.hap_share.clear();
-  if (sharing) c.hap_share.assign((size_t)(c.hb - c.ha), -1);
+  c.hap_order.clear();
+  if (sharing) {
+    c.hap_share.assign((size_t)(c.hb - c.ha), -1);
+    c.hap_order.assign((size_t)(c.hb - c.ha), 0);
+  }
   parallel_for(nslices, 1, [&](int64_t s_lo, int64_t s_hi) {
    for (int64_t si = s_lo; si < s_hi; ++si) {
     Slice& sl = slices[(size_t)si];
@@ -527,7 +550,9 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
     const int64_t h_lo = b->region_hap_off[g], h_hi = b->region_hap_off[g + 1];
     const int64_t nh = h_hi - h_lo;
     const int64_t region_out = region_out_of[g - g0];
-    if (sharing) region_shares(b, h_lo, h_hi, c.hap_share.data() + (h_lo - c.ha));
+    if (sharing)
+      region_order_and_shares(b, h_lo, h_hi, c.ha, c.hap_order.data() + (h_lo - c.ha),
+                              c.hap_share.data() + (h_lo - c.ha));
     // emit the haplotype runs of read r (and r2 >= 0 riding along)
     auto emit = [&](int64_t r, int64_t r2) {
       const int32_t code = c.read_code[r - c.ra];
@@ -538,17 +563,22 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       const int n_rows = n + (anchored ? 1 : 0);
       const int64_t rows = (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R));
       const bool multistrip = n_rows > kStripRows;
+      // two-read items walk the region in its lexicographic order: position
+      // i (global numbering) holds haplotype hap_at(i)
+      const bool sorted = r2 >= 0 && sharing;
+      auto hap_at = [&](int64_t i) -> int64_t { return sorted ? c.ha + c.hap_order[i - c.ha] : i; };
+      auto len_at = [&](int64_t i) -> int { const int64_t x = hap_at(i); return (int)(b->hap_off[x + 1] - b->hap_off[x]); };
       int64_t h = h_lo;
       while (h < h_hi) {
-        const int m0 = (int)(b->hap_off[h + 1] - b->hap_off[h]);
+        const int m0 = len_at(h);
         if (m0 <= 0) { ++h; continue; }
         int64_t run_end = h, stream = 0;
         while (run_end < h_hi) {
-          const int m = (int)(b->hap_off[run_end + 1] - b->hap_off[run_end]);
+          const int m = len_at(run_end);
           if (m <= 0) break;
           // a haplotype after the first of a two-read run streams only the
           // columns past its shared prefix
-          const int col0 = (r2 >= 0 && run_end > h && sharing) ? c.hap_share[run_end - c.ha] + 1 : 0;
+          const int col0 = (sorted && run_end > h) ? c.hap_share[run_end - c.ha] + 1 : 0;
           if (run_end > h && (plain || multistrip || stream + m + 1 - col0 > kMaxStream)) break;
           stream += m + 1 - col0;
           sl.cells += (int64_t)(n + n2) * m;
@@ -560,10 +590,12 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
         w.read = (int32_t)(r - c.ra);
         w.nhap = (int32_t)(run_end - h);
         w.hap_begin = h - c.ha;
-        w.out_begin = region_out + (r - r_lo) * nh + (h - h_lo);
+        // sorted: output slot = out_begin + hap_order[position] (the chunk-local haplotype)
+        const int64_t col = sorted ? -(h_lo - c.ha) : (h - h_lo);
+        w.out_begin = region_out + (r - r_lo) * nh + col;
         w.code = r2 >= 0 ? (item_code | kPairedBit) : item_code;
         w.read2 = r2 >= 0 ? (int32_t)(r2 - c.ra) : -1;
-        w.out2_begin = r2 >= 0 ? region_out + (r2 - r_lo) * nh + (h - h_lo) : 0;
+        w.out2_begin = r2 >= 0 ? region_out + (r2 - r_lo) * nh + col : 0;
         items.push_back(w);
         cost.push_back(rows * (stream + kWarp) * (r2 >= 0 ? 2 : 1));
         h = run_end;
@@ -689,8 +721,8 @@ void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64
 
 // Device bytes a chunk needs (inputs, lists, outputs, rescue lists, scratch).
 struct Layout {
-  size_t o_rb, o_rq, o_roff, o_rcode, o_hb, o_hoff, o_hsel, o_osel, o_hshare, o_items, o_out, o_sp1, o_sp2,
-      o_cnt, o_scratch, total;
+  size_t o_rb, o_rq, o_roff, o_rcode, o_hb, o_hoff, o_hsel, o_osel, o_hord, o_hshare, o_items, o_out, o_sp1,
+      o_sp2, o_cnt, o_scratch, total;
   int64_t scratch_stride;  // double2 records per warp slot
   int64_t warps;
 };
@@ -709,6 +741,7 @@ Layout layout_for(const HostChunk& c, const vd_batch* b, int64_t warps) {
   L.o_hoff = take(c.hap_off.size() * sizeof(int64_t));
   L.o_hsel = take(c.hap_sel.size() * sizeof(int32_t));
   L.o_osel = take(c.out_sel.size() * sizeof(int64_t));
+  L.o_hord = take(c.hap_order.size() * sizeof(int32_t));
   L.o_hshare = take(c.hap_share.size() * sizeof(int32_t));
   L.o_items = take(c.items.size() * sizeof(WorkItem));
   L.o_out = take((size_t)c.n_out * sizeof(double));
@@ -803,6 +836,7 @@ BatchView batch_view(vd_plan* pl) {
   bv.hap_sel = pl->chunk.hap_sel.empty() && pl->chunk.out_sel.empty() ? nullptr : (const int32_t*)(d + pl->L.o_hsel);
   bv.out_sel = bv.hap_sel ? (const int64_t*)(d + pl->L.o_osel) : nullptr;
   bv.hap_share = pl->chunk.hap_share.empty() ? nullptr : (const int32_t*)(d + pl->L.o_hshare);
+  bv.hap_order = pl->chunk.hap_order.empty() ? nullptr : (const int32_t*)(d + pl->L.o_hord);
   bv.out = (double*)(d + pl->L.o_out);
   return bv;
 }
@@ -829,6 +863,7 @@ int upload_chunk(vd_plan* pl, const vd_batch* b, int64_t* h2d) {
   if ((rc = put(pl->L.o_hoff, c.hap_off.data(), c.hap_off.size() * sizeof(int64_t)))) return rc;
   if ((rc = put(pl->L.o_hsel, c.hap_sel.data(), c.hap_sel.size() * sizeof(int32_t)))) return rc;
   if ((rc = put(pl->L.o_osel, c.out_sel.data(), c.out_sel.size() * sizeof(int64_t)))) return rc;
+  if ((rc = put(pl->L.o_hord, c.hap_order.data(), c.hap_order.size() * sizeof(int32_t)))) return rc;
   if ((rc = put(pl->L.o_hshare, c.hap_share.data(), c.hap_share.size() * sizeof(int32_t)))) return rc;
   if ((rc = put(pl->L.o_items, c.items.data(), c.items.size() * sizeof(WorkItem)))) return rc;
   if (c.n_out > 0) {

@@ -534,6 +534,14 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   auto share_of = [&](int k) -> int {
     return (k > 0 && k < K && bv.hap_share != nullptr) ? (int)bv.hap_share[w.hap_begin + k] : -1;
   };
+  // haplotype k of the item and its output column: through hap_order when the
+  // region's haplotypes are visited in lexicographic order
+  auto col_of = [&](int k) -> int64_t {
+    return bv.hap_order != nullptr ? (int64_t)bv.hap_order[w.hap_begin + k] : (int64_t)k;
+  };
+  auto hap_of = [&](int k) -> int64_t {
+    return bv.hap_order != nullptr ? (int64_t)bv.hap_order[w.hap_begin + k] : w.hap_begin + k;
+  };
   int kL = -1, next_reset = 0, S_cur = -1, c0 = 0, save_at = -1;
   const uint8_t* hp = bv.hap_bases;
   float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
@@ -543,11 +551,11 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   double* const svd = reinterpret_cast<double*>(sv + (3 * R + 2) * kWarp);
 
   auto finalize = [&](int k) {
-    const int64_t h = w.hap_begin + k;
+    const int64_t h = hap_of(k);
     const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
     const double lnC0 = sc.ln_c + log((double)(m + 1));
     const double za = accA + (double)acc32.x, zb = accB + (double)acc32.y;
-    const int64_t oa = w.out_begin + k, ob = w.out2_begin + k;
+    const int64_t oa = w.out_begin + col_of(k), ob = w.out2_begin + col_of(k);
     if (za >= (double)sc.final_floor && za < HUGE_VAL) {
       bv.out[oa] = log(za) - lnC0 + lnA;
     } else {
@@ -618,7 +626,7 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
           acc32 = make_float2(0.f, 0.f);
           accA = accB = 0.0;
         }
-        const int64_t h = w.hap_begin + kL;
+        const int64_t h = hap_of(kL);
         const int64_t ho = bv.hap_off[h];
         hp = bv.hap_bases + ho + c0 - 1 - p;
         next_reset = p + (int)(bv.hap_off[h + 1] - ho) + 1 - c0;
@@ -657,7 +665,8 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   for (int k = 0; k <= K; ++k) {
     int seg = 0, ck = 0, w0 = -1;
     if (k < K) {
-      const int mk = (int)(bv.hap_off[w.hap_begin + k + 1] - bv.hap_off[w.hap_begin + k]);
+      const int64_t hk = hap_of(k);
+      const int mk = (int)(bv.hap_off[hk + 1] - bv.hap_off[hk]);
       ck = share_of(k) + 1;
       seg = mk + 1 - ck;
       const int qn = share_of(k + 1);
