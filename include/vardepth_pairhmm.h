@@ -132,7 +132,11 @@ typedef struct vd_tuning {
   int pair_mask;        /* bit R (1..8): two reads with R rows per lane may share a warp in the
                            packed FP32 kernel (default 0x1fe: every R) */
   int max_item_columns; /* haplotype columns one work item streams at most; 0 = unlimited (default) */
-  int reserved[5];      /* must be zero */
+  int pipeline_gcells;  /* vd_forward cuts a batch of N >= 2 x this many 1e9 DP cells into
+                           min(8, N / this) chunks (the first a quarter of the others), so the
+                           host work and copies of one chunk overlap the kernels of the previous
+                           one; 0 = the default (300), 1e6 or more = one chunk */
+  int reserved[4];      /* must be zero */
 } vd_tuning;
 int vd_engine_set_tuning(vd_engine *engine, const vd_tuning *tuning);
 int vd_engine_get_tuning(const vd_engine *engine, vd_tuning *tuning);

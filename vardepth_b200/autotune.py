@@ -56,8 +56,13 @@ def signature(read_off, hap_off) -> str:
     return f"reads[{f(rb)}] haps[{f(hb)}]"
 
 
+def _apply(engine: native.Engine, setting: dict) -> None:
+    """Set the tuned knobs, keeping the engine's other tuning fields."""
+    engine.set_tuning(**dict(engine.tuning(), **{k: setting[k] for k in DEFAULT}))
+
+
 def _time(engine: native.Engine, packed: native.Packed, params, setting: dict, repeats: int) -> float:
-    engine.set_tuning(**setting)
+    _apply(engine, setting)
     plan = engine.plan(packed, params)
     try:
         plan.run()  # captures the graph
@@ -80,7 +85,7 @@ def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int 
             cache = {}
     if use_cache and key in cache:
         best = cache[key]
-        engine.set_tuning(**best)
+        _apply(engine, best)
         return dict(best, cached=True)
     best = dict(DEFAULT)
     best_ms = _time(engine, packed, params, best, repeats)
@@ -94,7 +99,7 @@ def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int 
             trials.append((cand, ms))
             if ms < best_ms * 0.99:
                 best, best_ms = cand, ms
-    engine.set_tuning(**best)
+    _apply(engine, best)
     if log is not None:
         log.extend({"setting": t, "ms": round(ms, 3)} for t, ms in trials)
     if use_cache:

@@ -173,7 +173,7 @@ struct vd_engine {
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair[2] = {0, 0};          // blocks of the two-read kernels [wide]
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
-  vd_tuning tuning{256, 0x1fe, 0, {0, 0, 0, 0, 0}};  // vd_engine_set_tuning
+  vd_tuning tuning{256, 0x1fe, 0, 0, {0, 0, 0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
   DevBuf geno_arena;                  // buffers of vd_region_genotypes
   // table cache
@@ -1189,7 +1189,8 @@ int vd_engine_set_tuning(vd_engine* e, const vd_tuning* t) {
     return fail(VD_EINVAL, "long_read_rows must be 64, 128 or 256");
   if (t->pair_mask & ~0x1fe) return fail(VD_EINVAL, "pair_mask holds bits 1..8 only");
   if (t->max_item_columns < 0) return fail(VD_EINVAL, "max_item_columns must be >= 0");
-  for (int i = 0; i < 5; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  if (t->pipeline_gcells < 0) return fail(VD_EINVAL, "pipeline_gcells must be >= 0");
+  for (int i = 0; i < 4; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
   std::lock_guard<std::mutex> lk(e->mu);
   e->tuning = *t;
   return VD_OK;
@@ -1251,8 +1252,10 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   };
   int64_t total_cells = 0;
   for (int64_t u = 0; u < units; ++u) total_cells += unit_cells(u);
-  constexpr int64_t kPipelineCells = 150'000'000'000LL;  // ~50 ms of kernel time per chunk
-  const int64_t n_pipe = std::max<int64_t>(1, std::min<int64_t>(8, total_cells / kPipelineCells));
+  // The first chunk is a quarter of the others: its host work and upload are
+  // the only ones not hidden behind kernels.
+  const int64_t pipeline_cells = (int64_t)(e->tuning.pipeline_gcells > 0 ? e->tuning.pipeline_gcells : 300) * 1'000'000'000LL;
+  const int64_t n_pipe = std::max<int64_t>(1, std::min<int64_t>(8, total_cells / pipeline_cells));
   const int64_t chunk_cells = n_pipe > 1 ? (total_cells + n_pipe - 1) / n_pipe : INT64_MAX;
 
   int64_t fixed = pair_form ? (b->hap_off[b->n_haps] - b->hap_off[0]) + 8 * b->n_haps : 0;
@@ -1281,11 +1284,16 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   };
 
   int64_t u = 0, chunk_index = 0;
+  // The primary tier of a chunk waits for the primary tier of the previous
+  // chunk (its copies do not): FP32 kernels of two chunks sharing the SMs run
+  // different variants side by side and thrash the instruction cache.  The
+  // FP64 rescue tiers, a few warps each, overlap the next chunk.
+  cudaEvent_t prev_primary = nullptr;
   while (u < units) {
     int64_t u_end = u, bytes = fixed, cells = 0;
     while (u_end < units) {
       const int64_t ub = unit_bytes(u_end);
-      if (u_end > u && (bytes + ub > budget || cells >= chunk_cells)) break;
+      if (u_end > u && (bytes + ub > budget || cells >= (chunk_index == 0 ? chunk_cells / 4 : chunk_cells))) break;
       bytes += ub;
       cells += unit_cells(u_end);
       ++u_end;
@@ -1315,8 +1323,10 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     pl.base = (char*)sl.arena.p;
     s.live_bytes = std::max<int64_t>(s.live_bytes, (int64_t)(e->slots[0].arena.bytes + e->slots[1].arena.bytes));
     if ((rc = upload_chunk(&pl, b, &s.h2d_bytes))) return rc;
+    if (prev_primary) VD_CUDA(cudaStreamWaitEvent(pl.stream, prev_primary, 0));
     int launches = 0;
     if ((rc = enqueue_tiers(&pl, &launches))) return rc;
+    prev_primary = pl.ev_mid;
     s.kernel_launches += launches + (c.n_out > 0 ? 1 : 0);  // the -inf fill of the upload
     const double* dout = (const double*)(pl.base + pl.L.o_out);
     if (c.n_out > 0) {

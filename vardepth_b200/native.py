@@ -55,11 +55,11 @@ class VdStats(ctypes.Structure):
 
 class VdTuning(ctypes.Structure):
     _fields_ = [("long_read_rows", ctypes.c_int), ("pair_mask", ctypes.c_int), ("max_item_columns", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("pipeline_gcells", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
     def as_dict(self) -> dict:
         return {"long_read_rows": self.long_read_rows, "pair_mask": self.pair_mask,
-                "max_item_columns": self.max_item_columns}
+                "max_item_columns": self.max_item_columns, "pipeline_gcells": self.pipeline_gcells}
 
 
 class VdGenotypeOptions(ctypes.Structure):
@@ -255,9 +255,11 @@ class Engine:
         check(library().vd_engine_get_tuning(self.handle, ctypes.byref(t)), "vd_engine_get_tuning")
         return t.as_dict()
 
-    def set_tuning(self, long_read_rows: int = 256, pair_mask: int = 0x1FE, max_item_columns: int = 0) -> None:
+    def set_tuning(self, long_read_rows: int = 256, pair_mask: int = 0x1FE, max_item_columns: int = 0,
+                   pipeline_gcells: int = 0) -> None:
         t = VdTuning()
         t.long_read_rows, t.pair_mask, t.max_item_columns = int(long_read_rows), int(pair_mask), int(max_item_columns)
+        t.pipeline_gcells = int(pipeline_gcells)
         check(library().vd_engine_set_tuning(self.handle, ctypes.byref(t)), "vd_engine_set_tuning")
 
     def forward(self, packed: Packed, params: VdParams, out: np.ndarray | None = None):
