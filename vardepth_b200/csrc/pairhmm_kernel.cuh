@@ -459,10 +459,28 @@ __device__ __forceinline__ float2 shfl_up2(float2 v) {
   return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
 }
 
+// What a lane needs when it starts haplotype k of a two-read item, written
+// once per haplotype by the whole warp into a per-warp ring of kMetaRing
+// entries, so the lane that starts it (one lane per step of the ramp) reads
+// shared memory instead of a chain of dependent global loads.  A lane starts
+// haplotype k at most 31 steps after the warp wrote its entry and lane 31
+// finalises it at most 31 steps after that, while the entry is overwritten
+// only kMetaRing haplotypes (at least kMetaRing steps) later.
+struct HapMeta {
+  int64_t ho;     // offset of its bases
+  double lnC0;    // ln c + ln(m + 1): the row-0 constant and the free-start count
+  int32_t h;      // chunk-local haplotype
+  int32_t m;      // length
+  int32_t q;      // shared prefix column (-1: none)
+  int32_t qn;     // shared prefix column of the next haplotype of the item
+  int64_t col;    // output column (added to out_begin / out2_begin)
+};
+constexpr int kMetaRing = 64;
+
 template <int R>
 __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv, const ItemRef it,
                                           const Tables<float>* __restrict__ tb, const Scalars<float> sc,
-                                          const int lane, float2* __restrict__ sv) {
+                                          const int lane, float2* __restrict__ sv, HapMeta* __restrict__ ring) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr double kLn2 = 0.6931471805599453094;
   const WorkItem& w = it.w;
@@ -550,12 +568,28 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   // row, s_top, the FP32 row sums, then the two FP64 row sums
   double* const svd = reinterpret_cast<double*>(sv + (3 * R + 2) * kWarp);
 
+  // the warp writes haplotype k's ring entry (every lane computes it, lane 0
+  // stores it)
+  auto publish = [&](int k) -> HapMeta {
+    HapMeta e;
+    e.h = (int32_t)hap_of(k);
+    e.ho = bv.hap_off[e.h];
+    e.m = (int32_t)(bv.hap_off[e.h + 1] - e.ho);
+    e.q = share_of(k);
+    e.qn = share_of(k + 1);
+    e.col = col_of(k);
+    e.lnC0 = sc.ln_c + log((double)(e.m + 1));
+    if (lane == 0) ring[k & (kMetaRing - 1)] = e;
+    __syncwarp();
+    return e;
+  };
+
   auto finalize = [&](int k) {
-    const int64_t h = hap_of(k);
-    const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
-    const double lnC0 = sc.ln_c + log((double)(m + 1));
+    const HapMeta& e = ring[k & (kMetaRing - 1)];
+    const int64_t h = e.h;
+    const double lnC0 = e.lnC0;
     const double za = accA + (double)acc32.x, zb = accB + (double)acc32.y;
-    const int64_t oa = w.out_begin + col_of(k), ob = w.out2_begin + col_of(k);
+    const int64_t oa = w.out_begin + e.col, ob = w.out2_begin + e.col;
     if (za >= (double)sc.final_floor && za < HUGE_VAL) {
       bv.out[oa] = log(za) - lnC0 + lnA;
     } else {
@@ -611,7 +645,8 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
       S_cur = p;
       save_at = -1;
       if (kL < K) {
-        const int q = share_of(kL);
+        const HapMeta& e = ring[kL & (kMetaRing - 1)];
+        const int q = e.q;
         c0 = q + 1;
         if (q >= 0) {
           restore();
@@ -626,13 +661,11 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
           acc32 = make_float2(0.f, 0.f);
           accA = accB = 0.0;
         }
-        const int64_t h = hap_of(kL);
-        const int64_t ho = bv.hap_off[h];
-        hp = bv.hap_bases + ho + c0 - 1 - p;
-        next_reset = p + (int)(bv.hap_off[h + 1] - ho) + 1 - c0;
+        hp = bv.hap_bases + e.ho + c0 - 1 - p;
+        next_reset = p + e.m + 1 - c0;
         // the next haplotype starts from column qn: a snapshot of it is taken
         // here, or (qn == c0 - 1) the one this haplotype started from stays
-        const int qn = share_of(kL + 1);
+        const int qn = e.qn;
         if (qn >= c0) save_at = p + (qn - c0);
       } else {
         next_reset = INT_MAX;
@@ -665,12 +698,10 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   for (int k = 0; k <= K; ++k) {
     int seg = 0, ck = 0, w0 = -1;
     if (k < K) {
-      const int64_t hk = hap_of(k);
-      const int mk = (int)(bv.hap_off[hk + 1] - bv.hap_off[hk]);
-      ck = share_of(k) + 1;
-      seg = mk + 1 - ck;
-      const int qn = share_of(k + 1);
-      if (qn >= ck) w0 = S + (qn - ck);  // lanes take the snapshot at steps w0 .. w0 + 31
+      const HapMeta e = publish(k);
+      ck = e.q + 1;
+      seg = e.m + 1 - ck;
+      if (e.qn >= ck) w0 = S + (e.qn - ck);  // lanes take the snapshot at steps w0 .. w0 + 31
     }
     const int Snext = S + seg;
     const int gen_end = (k < K) ? min(S + kWarp, Snext) : S + kWarp;
@@ -809,6 +840,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
   __shared__ Tables<float> tab;
   // per warp: the lane states laid down at a shared haplotype prefix
   __shared__ float2 saves[kWarpsPerBlock][(3 * kHiR + 4) * kWarp];
+  __shared__ HapMeta meta[kWarpsPerBlock][kMetaRing];
   {
     const int words = (int)(sizeof(Tables<float>) / sizeof(int));
     const int* src = reinterpret_cast<const int*>(gtab);
@@ -829,7 +861,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
     it.tier = 0;
     switch (code_R(it.w.code)) {
 #define VD_PCASE(r) \
-      case r: if constexpr (r >= kLoR && r <= kHiR) process_pair<r>(bv, qv, it, &tab, sc, lane, sv); break;
+      case r: if constexpr (r >= kLoR && r <= kHiR) process_pair<r>(bv, qv, it, &tab, sc, lane, sv, meta[threadIdx.x >> 5]); break;
       VD_PCASE(1) VD_PCASE(2) VD_PCASE(3) VD_PCASE(4) VD_PCASE(5) VD_PCASE(6) VD_PCASE(7) VD_PCASE(8)
 #undef VD_PCASE
       default: break;
