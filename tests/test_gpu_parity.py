@@ -225,6 +225,25 @@ def test_pairs_regions_and_chunking_agree():
     np.testing.assert_array_equal(chunked_pairs, regions)
 
 
+def test_pipelined_chunks_agree():
+    """vd_forward's pipelined chunks (the first a quarter of the others, each chunk's
+    primary tier ordered after the previous one's) give the single-chunk results bit for bit."""
+    w = S.config1(n_regions=300)
+    eng = native.Engine(0, 8192)
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    eng.set_tuning(pipeline_gcells=1_000_000)
+    one, st1 = eng.forward(_packed(w), params)
+    assert st1.batches == 1
+    eng.set_tuning(pipeline_gcells=max(1, w.cells() // 6 // 10**9))
+    assert eng.tuning()["pipeline_gcells"] >= 1
+    many, stn = eng.forward(_packed(w), params)
+    assert stn.batches >= 4 and stn.shared_cells == st1.shared_cells
+    np.testing.assert_array_equal(many, one)
+    with pytest.raises(ValueError):
+        eng.set_tuning(pipeline_gcells=-1)
+    eng.close()
+
+
 def test_plan_graph_replay_is_deterministic():
     w = S.config1(n_regions=16)
     eng = native.Engine(0, 4096)
