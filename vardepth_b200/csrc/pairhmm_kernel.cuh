@@ -711,7 +711,11 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
       // snapshot window of the next haplotype runs through gstep
       while (t < Snext) {
         if (w0 >= 0 && t >= w0 && t < w0 + kWarp) {
-          gstep(t);
+          // no lane starts a haplotype here: a column step, lane 31's flush
+          // by column and the snapshot of the lane whose turn it is
+          sstep((uint32_t)hp[t - lane]);
+          if (((ck - (kWarp - 1) - S + t) & 7) == 7) flush();
+          if (t - lane == save_at) save();
           ++t;
           continue;
         }
