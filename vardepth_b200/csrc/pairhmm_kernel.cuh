@@ -480,7 +480,7 @@ constexpr int kMetaRing = 64;
 template <int R>
 __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv, const ItemRef it,
                                           const Tables<float>* __restrict__ tb, const Scalars<float> sc,
-                                          const int lane, float2* __restrict__ sv, HapMeta* __restrict__ ring) {
+                                          const int lane, float4* __restrict__ sv, HapMeta* __restrict__ ring) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr double kLn2 = 0.6931471805599453094;
   const WorkItem& w = it.w;
@@ -564,9 +564,12 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   const uint8_t* hp = bv.hap_bases;
   float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
   double accA = 0.0, accB = 0.0;
-  // snapshot layout, slot-major with one entry per lane: mu, om, s of every
-  // row, s_top, the FP32 row sums, then the two FP64 row sums
-  double* const svd = reinterpret_cast<double*>(sv + (3 * R + 2) * kWarp);
+  // snapshot layout, 16-byte entries slot-major with one entry per lane (the
+  // lane that saves or restores is alone in its branch, so its instruction
+  // count is what costs): (mu, om) of each row, s of two rows, (s_top, FP32
+  // row sums), the two FP64 row sums
+  constexpr int kSPairs = (R + 1) / 2;
+  double2* const svd = reinterpret_cast<double2*>(sv + (R + kSPairs + 1) * kWarp);
 
   // the warp writes haplotype k's ring entry (every lane computes it, lane 0
   // stores it)
@@ -611,27 +614,35 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   };
   auto save = [&]() {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      sv[(3 * r) * kWarp + lane] = rw.mu[r];
-      sv[(3 * r + 1) * kWarp + lane] = rw.om[r];
-      sv[(3 * r + 2) * kWarp + lane] = rw.s[r];
+    for (int r = 0; r < R; ++r)
+      sv[r * kWarp + lane] = make_float4(rw.mu[r].x, rw.mu[r].y, rw.om[r].x, rw.om[r].y);
+#pragma unroll
+    for (int r = 0; r < R; r += 2) {
+      const float2 b = (r + 1 < R) ? rw.s[r + 1] : make_float2(0.f, 0.f);
+      sv[(R + r / 2) * kWarp + lane] = make_float4(rw.s[r].x, rw.s[r].y, b.x, b.y);
     }
-    sv[3 * R * kWarp + lane] = s_top;
-    sv[(3 * R + 1) * kWarp + lane] = acc32;
-    svd[lane] = accA;
-    svd[kWarp + lane] = accB;
+    sv[(R + kSPairs) * kWarp + lane] = make_float4(s_top.x, s_top.y, acc32.x, acc32.y);
+    svd[lane] = make_double2(accA, accB);
   };
   auto restore = [&]() {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      rw.mu[r] = sv[(3 * r) * kWarp + lane];
-      rw.om[r] = sv[(3 * r + 1) * kWarp + lane];
-      rw.s[r] = sv[(3 * r + 2) * kWarp + lane];
+      const float4 v = sv[r * kWarp + lane];
+      rw.mu[r] = make_float2(v.x, v.y);
+      rw.om[r] = make_float2(v.z, v.w);
     }
-    s_top = sv[3 * R * kWarp + lane];
-    acc32 = sv[(3 * R + 1) * kWarp + lane];
-    accA = svd[lane];
-    accB = svd[kWarp + lane];
+#pragma unroll
+    for (int r = 0; r < R; r += 2) {
+      const float4 v = sv[(R + r / 2) * kWarp + lane];
+      rw.s[r] = make_float2(v.x, v.y);
+      if (r + 1 < R) rw.s[r + 1] = make_float2(v.z, v.w);
+    }
+    const float4 v = sv[(R + kSPairs) * kWarp + lane];
+    s_top = make_float2(v.x, v.y);
+    acc32 = make_float2(v.z, v.w);
+    const double2 a = svd[lane];
+    accA = a.x;
+    accB = a.y;
   };
 
   // step with per-lane haplotype bookkeeping (ramps, snapshots, short haplotypes)
@@ -843,7 +854,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
                     const Scalars<float> sc) {
   __shared__ Tables<float> tab;
   // per warp: the lane states laid down at a shared haplotype prefix
-  __shared__ float2 saves[kWarpsPerBlock][(3 * kHiR + 4) * kWarp];
+  __shared__ float4 saves[kWarpsPerBlock][(kHiR + (kHiR + 1) / 2 + 2) * kWarp];
   __shared__ HapMeta meta[kWarpsPerBlock][kMetaRing];
   {
     const int words = (int)(sizeof(Tables<float>) / sizeof(int));
@@ -853,7 +864,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
   }
   __syncthreads();
   const int lane = threadIdx.x & (kWarp - 1);
-  float2* sv = saves[threadIdx.x >> 5];
+  float4* sv = saves[threadIdx.x >> 5];
   for (;;) {
     unsigned long long i = 0;
     if (lane == 0) i = atomicAdd(qv.head, 1ull);
