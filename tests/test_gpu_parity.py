@@ -252,7 +252,8 @@ def test_plan_graph_replay_is_deterministic():
     outs = []
     for _ in range(3):
         st = plan.run()
-        assert st.kernel_launches in (3, 4, 5) and st.pairs == w.pairs()
+        # two-read kernels (1-2), single reads, drift, FP64, FP64 strips
+        assert st.kernel_launches in (4, 5, 6) and st.pairs == w.pairs()
         outs.append(plan.fetch())
     ref, _ = eng.forward(_packed(w), params)
     for o in outs:
@@ -374,10 +375,14 @@ def test_long_read_strip_heights(rows, anchored):
             np.testing.assert_allclose(got, want, rtol=0, atol=FP64_ATOL_LN * 10)
         else:
             assert_mixed_close(got, want)
-            if rows == 64 and not anchored:
-                # anchored pairs here force 120+ deletions (likelihoods far below the FP32
-                # range whatever the strip height) and are rescued in FP64 by design
+            if not anchored:
+                # the error-rich reads leave a 256-row FP32 strip's range; the drift tier
+                # (per-row power-of-two boosts) resolves them in FP32 at every strip
+                # height.  Anchored pairs here force 120+ deletions (likelihoods far below
+                # the FP32 range) and are rescued in FP64 by design.
                 assert st.rescued_fp64 + st.rescued_robust == 0
+                if rows == 256:
+                    assert st.rescued_fp32 > 0
     with pytest.raises(ValueError):
         eng.set_tuning(long_read_rows=96)
     eng.close()

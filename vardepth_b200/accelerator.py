@@ -175,6 +175,7 @@ class CudaPairHMM:
                          float64_fallback_backend=("cuda_float64" if rescued else None),
                          float64_fallback_pairs=int(rescued),
                          float64_robust_pairs=int(s["rescued_robust"]),
+                         float32_drift_pairs=int(s["rescued_fp32"]),
                          pairs=int(s["pairs"]), dp_cells=int(s["dp_cells"]), batches=int(s["batches"]),
                          work_items=int(s["work_items"]), live_array_bytes_upper_bound=int(s["live_bytes"]),
                          seconds=time.perf_counter() - start, includes_packing_transfers_and_synchronization=True,

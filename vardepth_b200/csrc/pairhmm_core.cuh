@@ -40,6 +40,7 @@ constexpr int kWarp = 32;
 constexpr int kMaxR = 8;                       // read rows per lane
 constexpr int kStripRows = kWarp * kMaxR;      // rows per strip of a long read
 constexpr int kWarpsPerBlock = 4;
+constexpr int kDriftTier = 3;  // tier number of the FP32 drift-compensated rescue (pairhmm_kernel.cuh)
 
 // Work item: one read against a list of haplotypes.
 struct WorkItem {
@@ -85,6 +86,7 @@ struct Scalars {
   T k2, x, gfin, c;          // c: value of the row-0 cells (power of two)
   double ln_c;               // ln c
   T strip_floor;             // below this a strip boundary counts as underflowed
+  T strip_ceil;              // at or above this it counts as overflowed (+inf: only inf / NaN)
   T final_floor;             // below this the final scaled sum counts as underflowed
   int target_log2;           // strip boundary maxima are renormalised to 2^target
 };

@@ -88,6 +88,7 @@ struct TableSet {
   Tables<double> f64;
   Scalars<float> s32;
   Scalars<double> s64;
+  Scalars<float> s32d;  // the drift tier: row 0 = 1, strips brought to 2^0, window 2^-60 .. 2^60
 };
 
 // Per-quality factors of the scaled recurrence (pairhmm_core.cuh).  The error
@@ -119,10 +120,20 @@ void build_tables(double g, double x, const double* offsets, TableSet* ts) {
   // sum >= 2^-80 keeps the dominant cells normal (>= 2^-93 after m+1 <= 2^13 terms)
   ts->s32.c = std::ldexp(1.0f, 120); ts->s32.ln_c = 120.0 * std::log(2.0);
   ts->s32.strip_floor = std::ldexp(1.0f, -40); ts->s32.final_floor = std::ldexp(1.0f, -80);
+  ts->s32.strip_ceil = HUGE_VALF;
   ts->s32.target_log2 = 120;
+  // the drift tier keeps every strip's bottom near 2^0 with per-row boosts, so
+  // it starts there and leaves 60 binary orders either side for what the
+  // boosts do not cancel
+  ts->s32d = ts->s32;
+  ts->s32d.c = 1.0f; ts->s32d.ln_c = 0.0;
+  ts->s32d.strip_floor = std::ldexp(1.0f, -60); ts->s32d.strip_ceil = std::ldexp(1.0f, 60);
+  ts->s32d.final_floor = std::ldexp(1.0f, -60);
+  ts->s32d.target_log2 = 0;
   ts->s64.k2 = k2; ts->s64.x = x; ts->s64.gfin = g;
   ts->s64.c = std::ldexp(1.0, 600); ts->s64.ln_c = 600.0 * std::log(2.0);
   ts->s64.strip_floor = std::ldexp(1.0, -800); ts->s64.final_floor = std::ldexp(1.0, -900);
+  ts->s64.strip_ceil = HUGE_VAL;
   ts->s64.target_log2 = 600;
 }
 
@@ -172,6 +183,7 @@ struct vd_engine {
   std::mutex mu;
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair[2] = {0, 0};          // blocks of the two-read kernels [wide]
+  int grid_drift = 0;                 // blocks of the drift tier (no more than grid[0][0])
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
   vd_tuning tuning{256, 0x1fe, 0, 0, {0, 0, 0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
@@ -888,7 +900,9 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   // as external; otherwise it would only order the capture
   const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   cudaGetLastError();  // launch checks below must see only their own errors
-  // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag
+  // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag,
+  // cnt[6..7] heads of the two-read kernels, cnt[8] spill count of the FP64
+  // tier and cnt[9] head of the drift tier (FP32 semiglobal only)
   VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), pl->stream));
   VD_CUDA(cudaEventRecordWithFlags(pl->ev_begin, pl->stream, evflags));
   const BatchView bv = batch_view(pl);
@@ -940,16 +954,34 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
     rv.hap_sel = nullptr;
     rv.out_sel = nullptr;
     q.static_order = 0;  // the rescue tiers always run on the shared counter
+    // the lists: tier 0 spills into sp1; with the drift tier (FP32
+    // semiglobal) the chain is sp1 -> drift -> sp2 -> FP64 -> sp1 (cnt[8]) ->
+    // robust, otherwise sp1 -> FP64 -> sp2 -> robust
+    const bool drift = !f64 && !anch;
     QueueView q1 = q;
+    if (drift) {
+      QueueView qd = q;
+      qd.items = nullptr;
+      qd.entries = (const RescueEntry*)(d + L.o_sp1);
+      qd.count = cnt + 3;
+      qd.n_items = cap;
+      qd.head = cnt + 9;
+      qd.spill = (RescueEntry*)(d + L.o_sp2);
+      qd.spill_count = cnt + 4;
+      qd.scratch_stride = 2 * L.scratch_stride;  // two float2 boundaries in each warp's double2 slot
+      err = launch_drift_f32(rv, qd, &dt->f32, ht->s32d, e->grid_drift, pl->stream);
+      if (err != cudaSuccess) return cuda_fail(err, "drift tier launch");
+      ++n;
+    }
     if (!f64) {
       // tier 1: FP64 wavefront over the FP32 spills
       q1.items = nullptr;
-      q1.entries = (const RescueEntry*)(d + L.o_sp1);
-      q1.count = cnt + 3;
+      q1.entries = (const RescueEntry*)(d + (drift ? L.o_sp2 : L.o_sp1));
+      q1.count = cnt + (drift ? 4 : 3);
       q1.n_items = cap;
       q1.head = cnt + 1;
-      q1.spill = (RescueEntry*)(d + L.o_sp2);
-      q1.spill_count = cnt + 4;
+      q1.spill = (RescueEntry*)(d + (drift ? L.o_sp1 : L.o_sp2));
+      q1.spill_count = cnt + (drift ? 8 : 4);
       err = launch_f64(anch, rv, q1, &dt->f64, ht->s64, 1, e->grid[1][anch], pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "rescue tier launch");
       ++n;
@@ -957,8 +989,8 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
     // tier 2: FP64 32-row strips over what the FP64 wavefront spilled
     QueueView q2 = q;
     q2.items = nullptr;
-    q2.entries = (const RescueEntry*)(d + (f64 ? L.o_sp1 : L.o_sp2));
-    q2.count = cnt + (f64 ? 3 : 4);
+    q2.entries = (const RescueEntry*)(d + ((f64 || drift) ? L.o_sp1 : L.o_sp2));
+    q2.count = cnt + (f64 ? 3 : drift ? 8 : 4);
     q2.n_items = cap;
     q2.head = cnt + 2;
     q2.spill = nullptr;
@@ -987,26 +1019,29 @@ int tier_times(const vd_plan* pl, double* total, double* primary, double* rescue
 }
 
 int enqueue_counter_read(vd_plan* pl, unsigned long long* host) {
-  VD_CUDA(cudaMemcpyAsync(host, pl->base + pl->L.o_cnt, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+  VD_CUDA(cudaMemcpyAsync(host, pl->base + pl->L.o_cnt, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                           pl->stream));
   return VD_OK;
 }
 
-// after the plan's stream completed
-int check_counters(const vd_plan* pl, const unsigned long long* h, int64_t* r1, int64_t* r2) {
+// after the plan's stream completed: pairs rescued by the drift tier (r0),
+// recomputed in the FP64 wavefront (r1) and in FP64 32-row strips (r2)
+int check_counters(const vd_plan* pl, const unsigned long long* h, int64_t* r0, int64_t* r1, int64_t* r2) {
   if (h[5]) return fail(VD_EOVERFLOW, "rescue list overflow");
   const bool f64 = pl->params.precision == VD_PRECISION_FLOAT64;
-  *r1 = f64 ? 0 : (int64_t)h[3];
-  *r2 = (int64_t)(f64 ? h[3] : h[4]);
+  const bool drift = !f64 && !pl->params.anchored;
+  *r0 = drift ? (int64_t)(h[3] - h[4]) : 0;
+  *r1 = f64 ? 0 : (int64_t)(drift ? h[4] : h[3]);
+  *r2 = (int64_t)(f64 ? h[3] : drift ? h[8] : h[4]);
   return VD_OK;
 }
 
-int read_counters(vd_plan* pl, int64_t* r1, int64_t* r2) {
-  unsigned long long h[6];
+int read_counters(vd_plan* pl, int64_t* r0, int64_t* r1, int64_t* r2) {
+  unsigned long long h[9];
   int rc = enqueue_counter_read(pl, h);
   if (rc) return rc;
   VD_CUDA(cudaStreamSynchronize(pl->stream));
-  return check_counters(pl, h, r1, r2);
+  return check_counters(pl, h, r0, r1, r2);
 }
 
 int init_engine_grids(vd_engine* e) {
@@ -1025,6 +1060,11 @@ int init_engine_grids(vd_engine* e) {
     if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
     e->grid_pair[wide] = std::max(1, bps) * e->sm_count;
   }
+  bps = 0;
+  err = occupancy_drift_f32(&bps);
+  if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+  // its warps index the strip scratch, which is sized by the largest grid
+  e->grid_drift = std::min(std::max(1, bps) * e->sm_count, e->grid[0][0]);
   for (int f = 0; f < 2; ++f) {
     bps = 0;
     err = occupancy_grad(f != 0, &bps);
@@ -1272,10 +1312,11 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     sl.busy = false;
     VD_CUDA(cudaStreamSynchronize(sl.stream));
     vd_plan& pl = *sl.pl;
-    int64_t r1 = 0, r2 = 0;
-    int r = check_counters(&pl, sl.hcnt, &r1, &r2);
+    int64_t r0 = 0, r1 = 0, r2 = 0;
+    int r = check_counters(&pl, sl.hcnt, &r0, &r1, &r2);
     if (r) return r;
     if ((r = tier_times(&pl, &s.kernel_ms, &s.primary_ms, &s.rescue_ms))) return r;
+    s.rescued_fp32 += r0;
     s.rescued_fp64 += r1;
     s.rescued_robust += r2;
     const HostChunk& c = pl.chunk;
@@ -1424,8 +1465,8 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
     launches = pl->graph_launches;
   }
   VD_CUDA(cudaGraphLaunch(pl->graph, e->stream));
-  int64_t r1 = 0, r2 = 0;
-  if ((rc = read_counters(pl, &r1, &r2))) return rc;
+  int64_t r0 = 0, r1 = 0, r2 = 0;
+  if ((rc = read_counters(pl, &r0, &r1, &r2))) return rc;
   double ms = 0.0, pms = 0.0, rms = 0.0;
   if ((rc = tier_times(pl, &ms, &pms, &rms))) return rc;
   pl->last_rescued1 = r1;
@@ -1437,6 +1478,7 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
     s.shared_cells = pl->chunk.shared_cells;
     s.work_items = (int64_t)pl->chunk.items.size();
     s.batches = 1;
+    s.rescued_fp32 = r0;
     s.rescued_fp64 = r1;
     s.rescued_robust = r2;
     s.kernel_launches = launches;

@@ -93,6 +93,17 @@ __device__ __forceinline__ void spill_pair(const QueueView& qv, int32_t read, in
 
 constexpr int kUnroll = 8;
 
+// The drift tier (FP32, semiglobal, reads longer than one strip) rescores the
+// pairs the primary tier spilled.  Error-rich long reads lose more per strip
+// than the FP32 range holds (8% errors at reported Q30: about 1 bit per row),
+// so each row's constants are multiplied by an exact power of two 2^k_i that
+// cancels the decay: Bs bits per strip, spread over its rows.  Bs is measured
+// as the read goes (the next strip takes the decay left over at the bottom of
+// this one) and a strip whose bottom leaves the window [2^-60, 2^60) is run
+// again with Bs corrected by the measured exponent (its input boundary is kept
+// in the other half of the warp's scratch).  What still fails goes to FP64.
+constexpr int kDriftTries = 6;
+
 // Row layout of one read (lane L, register r of strip s holds row
 // i = s*32R + L*R + r - v, 0-based):
 //  * semiglobal (v = 0): rows below the read pass the last row's u down the
@@ -105,7 +116,7 @@ constexpr int kUnroll = 8;
 //    row-0 deletions D[0][j] = g x^(j-1) (anchored.cpp:9).
 constexpr uint32_t kNeverBase = 0x10000u;  // compares unequal to every base byte
 
-template <typename T, int R, bool GEN, bool ANCH>
+template <typename T, int R, bool GEN, bool ANCH, bool DRIFT = false>
 __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv, const ItemRef it,
                                           const Tables<T>* __restrict__ tb, const Scalars<T> sc,
                                           const int lane, typename Vec2<T>::type* __restrict__ scratch) {
@@ -141,15 +152,27 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   int E = 0;          // total power-of-two renormalisation of the strips
   bool fail = false;  // a strip boundary underflowed
 
+  // drift tier: per-row power-of-two boosts, strips re-run when they leave the
+  // window; the scratch holds two boundaries (read one, write the other)
+  constexpr bool kCanDrift = DRIFT && std::is_same<T, float>::value && GEN && !ANCH;
+  constexpr bool drift = kCanDrift;
+  const long long half = drift ? qv.scratch_stride / 2 : qv.scratch_stride;
+  int strip_lg = 0;     // drift: exponent of the strip's bottom maximum (or +-1024: inf / zero)
+  double zkeep = 0.0;   // drift: the last strip's final sum, on lane 31
+
   // One strip of rows.  FIRST and LAST are compile-time tags, so the steady
   // loop carries no per-step test of the strip position.  Returns false when
   // the strip's bottom boundary underflowed.
-  auto run_strip = [&](auto first_tag, auto last_tag, const int strip) -> bool {
+  auto run_strip = [&](auto first_tag, auto last_tag, const int strip, const int Bs) -> bool {
     constexpr bool FIRST = decltype(first_tag)::value;
     constexpr bool last = decltype(last_tag)::value;
     const bool lane0 = lane == 0;
     LaneRows<T, R, GEN> rw;
     const int row0 = strip * SR + lane * R - v;
+    // the boundary this strip reads and the one it writes
+    T2* const src = scratch + (drift ? (long long)(strip & 1) * half : 0ll);
+    T2* const dst = scratch + (drift ? (long long)((strip + 1) & 1) * half : 0ll);
+    const int ns = min(SR, n - strip * SR);  // read rows of the strip (drift: semiglobal, v = 0)
     int emu = -1;  // register of the anchored row-0 emulator in this lane
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -161,6 +184,17 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         if (GEN) rw.hit[r] = tb->hit[q];
         rw.K[r] = tb->K[q];
         rw.X[r] = (!ANCH && i == n - 1) ? A : tb->X[q];
+        if constexpr (kCanDrift) {
+          {
+            // row il of the strip gets k = floor((il+1) Bs / ns) - floor(il Bs / ns)
+            const int il = i - strip * SR;
+            const T f = pow2T((il + 1) * Bs / ns - il * Bs / ns, T(0));
+            rw.miss[r] *= f;
+            rw.hit[r] *= f;
+            rw.K[r] *= f;
+            rw.X[r] *= f;
+          }
+        }
       } else {
         const bool emulator = ANCH && i == -1;
         if (emulator) emu = r;
@@ -193,6 +227,10 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       // than 1e-300 below that row maximum
       const double Zc = ANCH ? fmax(Zs, 1e-300 * (double)rmax) : Zs;
       const double lnC0 = sc.ln_c + (ANCH ? 0.0 : log((double)(m + 1)));
+      if constexpr (drift) {
+        zkeep = Zs;  // checked (and written) once the strip is done
+        return;
+      }
       const bool ok = !fail && Zs >= (double)sc.final_floor && Zs < HUGE_VAL;
       if (ok || qv.spill == nullptr) {
         bv.out[o] = (Zc > 0.0 ? log(Zc) : -HUGE_VAL) - lnC0 + lnN - (double)E * kLn2;
@@ -240,7 +278,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     T2 pf_cur = {T(0), T(0)}, pf_nxt = {T(0), T(0)};
     auto pf_load = [&](int base) -> T2 {
       const long long q = (long long)base + lane;
-      return q < qv.scratch_stride ? scratch[q] : T2{T(0), T(0)};
+      return q < half ? src[q] : T2{T(0), T(0)};
     };
     if (!FIRST) {
       pf_cur = pf_load(0);
@@ -303,7 +341,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         if (!ANCH && lane == kWarp - 1 && ((p - S_cur) & 7) == 7) { acc64 += (double)acc32; acc32 = T(0); }
       } else {
         if (lane == kWarp - 1 && active) {
-          scratch[p] = T2{rw.s[R - 1], u_bot};
+          dst[p] = T2{rw.s[R - 1], u_bot};
           bmax = maxT(bmax, maxT(rw.s[R - 1], u_bot));
         }
         __syncwarp();
@@ -331,7 +369,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       if (last) {
         accumulate(tmu, tnu, tom);
       } else if (lane == kWarp - 1) {
-        scratch[p] = T2{rw.s[R - 1], u_bot};
+        dst[p] = T2{rw.s[R - 1], u_bot};
         bmax = maxT(bmax, maxT(rw.s[R - 1], u_bot));
       }
     };
@@ -375,15 +413,20 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       // so that any exponent shift stays representable
       __syncwarp();
       const T bm = __shfl_sync(FULL, bmax, kWarp - 1);
-      if (!(bm >= sc.strip_floor) || !(bm < T(HUGE_VAL))) return false;
-      const int ks = sc.target_log2 - ilogb(bm);
+      if (!(bm >= sc.strip_floor) || !(bm < sc.strip_ceil)) {
+        // (1024: overflowed to inf or NaN, -1024: underflowed to zero)
+        strip_lg = (bm != bm || bm >= T(HUGE_VAL)) ? 1024 : (bm > T(0) ? ilogb(bm) : -1024);
+        return false;
+      }
+      strip_lg = ilogb(bm);
+      const int ks = sc.target_log2 - strip_lg;
       const int k1 = ks / 2;
       const T f1 = pow2T(k1, T(0)), f2 = pow2T(ks - k1, T(0));
       for (int p = lane; p < S - 1; p += kWarp) {
-        T2 v = scratch[p];
+        T2 v = dst[p];
         v.x = (v.x * f1) * f2;
         v.y = (v.y * f1) * f2;
-        scratch[p] = v;
+        dst[p] = v;
       }
       __syncwarp();
       E += ks;
@@ -391,12 +434,59 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     return true;
   };
 
-  if (nstrips == 1) {
-    run_strip(std::true_type{}, std::true_type{}, 0);
+  if constexpr (drift) {
+    // rescue entries carry one haplotype; single-strip reads go on to FP64
+    bool ok = nstrips > 1 && K == 1;
+    if constexpr (R == kMaxR || R == 4 || R == 2 || R == 1) {
+      int Bs = SR;  // first guess: one bit per row (the spilled reads lost more than 160 per strip)
+      for (int strip = 0; ok && strip < nstrips; ++strip) {
+        const int ns = min(SR, n - strip * SR);
+        for (int attempt = 0;; ++attempt) {
+          bool good;
+          if (strip == 0) {
+            good = run_strip(std::true_type{}, std::false_type{}, strip, Bs);
+          } else if (strip < nstrips - 1) {
+            good = run_strip(std::false_type{}, std::false_type{}, strip, Bs);
+          } else {
+            run_strip(std::false_type{}, std::true_type{}, strip, Bs);
+            const double z = __shfl_sync(FULL, zkeep, kWarp - 1);
+            good = z >= (double)sc.final_floor && z < (double)sc.strip_ceil;
+            strip_lg = (z != z || z >= HUGE_VAL) ? 1024 : (z > 0.0 ? ilogb(z) : -1024);
+          }
+          // bottom exponent above the target: the boosts were too strong
+          const int excess = strip_lg - sc.target_log2;
+          if (good) {
+            E += Bs;
+            if (strip + 1 < nstrips) {
+              // the next strip takes this one's rate plus what it left over
+              const int ns1 = min(SR, n - (strip + 1) * SR);
+              Bs = max(0, min(16 * ns1, (Bs - excess) * ns1 / ns));
+            }
+            break;
+          }
+          if (attempt + 1 == kDriftTries) {
+            ok = false;
+            break;
+          }
+          const int step = (strip_lg == 1024) ? -ns / 2 : (strip_lg == -1024) ? ns / 2 : -excess;
+          Bs = max(0, min(16 * ns, Bs + (step != 0 ? step : (excess > 0 ? -1 : 1))));
+        }
+      }
+      if (ok && lane == kWarp - 1) {
+        const int64_t h = hap_index(0);
+        const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
+        bv.out[out_index(0)] = log(zkeep) - (sc.ln_c + log((double)(m + 1))) + lnN - (double)E * kLn2;
+      }
+    } else {
+      ok = false;  // no strip-mined variant at this R: the pair goes on to FP64
+    }
+    fail = !ok;
+  } else if (nstrips == 1) {
+    run_strip(std::true_type{}, std::true_type{}, 0, 0);
   } else if constexpr (R == kMaxR || R == 4 || R == 2 || R == 1) {
-    bool ok = run_strip(std::true_type{}, std::false_type{}, 0);
-    for (int strip = 1; ok && strip < nstrips - 1; ++strip) ok = run_strip(std::false_type{}, std::false_type{}, strip);
-    if (ok) ok = run_strip(std::false_type{}, std::true_type{}, nstrips - 1);
+    bool ok = run_strip(std::true_type{}, std::false_type{}, 0, 0);
+    for (int strip = 1; ok && strip < nstrips - 1; ++strip) ok = run_strip(std::false_type{}, std::false_type{}, strip, 0);
+    if (ok) ok = run_strip(std::false_type{}, std::true_type{}, nstrips - 1, 0);
     fail = !ok;
   } else {
     fail = true;  // not reached: reads longer than one strip run with R = 8, 4 or 2 (1 in the robust tier)
@@ -880,6 +970,58 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
       VD_PCASE(1) VD_PCASE(2) VD_PCASE(3) VD_PCASE(4) VD_PCASE(5) VD_PCASE(6) VD_PCASE(7) VD_PCASE(8)
 #undef VD_PCASE
       default: break;
+    }
+  }
+}
+
+// The drift tier (FP32, semiglobal): the rescue list of the primary tier,
+// each entry in the two-sided emission form its boosted match factors need,
+// on its own kernel so the strip driver's state does not crowd the primary
+// kernel's registers (168 per thread, 3 blocks per SM).  Entries whose rows
+// per lane have no strip-mined variant go on to FP64 unchanged.
+template <int kBlocks>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
+pairhmm_drift_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
+                     const Scalars<float> sc) {
+  __shared__ Tables<float> tab;
+  {
+    const int words = (int)(sizeof(Tables<float>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(gtab);
+    int* dst = reinterpret_cast<int*>(&tab);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & (kWarp - 1);
+  const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  float2* scratch = reinterpret_cast<float2*>(qv.scratch) + gw * qv.scratch_stride;
+  long long total = qv.n_items;
+  const long long c = (long long)*qv.count;
+  total = c < total ? c : total;
+  for (;;) {
+    unsigned long long i = 0;
+    if (lane == 0) i = atomicAdd(qv.head, 1ull);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if ((long long)i >= total) break;
+    const RescueEntry e = qv.entries[i];
+    ItemRef it;
+    it.tier = kDriftTier;
+    it.use_sel = false;
+    it.w.read = e.read;
+    it.w.nhap = 1;
+    it.w.hap_begin = e.hap;
+    it.w.out_begin = e.out;
+    it.w.read2 = -1;
+    it.w.out2_begin = 0;
+    it.w.code = bv.read_code[e.read];
+    switch (code_R(it.w.code)) {
+      case 8: process_item<float, 8, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
+      case 4: process_item<float, 4, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
+      case 2: process_item<float, 2, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
+      case 1: process_item<float, 1, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
+      default:
+        if (lane == 0) spill_pair<float>(qv, e.read, e.hap, e.out);
+        __syncwarp();
+        break;
     }
   }
 }

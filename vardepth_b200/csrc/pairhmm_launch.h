@@ -14,6 +14,10 @@ cudaError_t occupancy_f64(bool anchored, int* blocks_per_sm);
 cudaError_t launch_pair_f32(bool wide, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                             const Scalars<float>& sc, int grid, cudaStream_t stream);
 cudaError_t occupancy_pair_f32(bool wide, int* blocks_per_sm);
+// the drift tier (FP32 semiglobal rescue with per-row power-of-two boosts)
+cudaError_t launch_drift_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
+                             const Scalars<float>& sc, int grid, cudaStream_t stream);
+cudaError_t occupancy_drift_f32(int* blocks_per_sm);
 // gradient kernel (pairhmm_backward.cuh), FP32 and FP64 passes
 struct GradTables;
 struct GradScalars;
