@@ -1325,11 +1325,13 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   };
 
   int64_t u = 0, chunk_index = 0;
-  // The primary tier of a chunk waits for the primary tier of the previous
-  // chunk (its copies do not): FP32 kernels of two chunks sharing the SMs run
-  // different variants side by side and thrash the instruction cache.  The
-  // FP64 rescue tiers, a few warps each, overlap the next chunk.
-  cudaEvent_t prev_primary = nullptr;
+  // The kernels of a chunk wait for all kernels of the previous chunk (its
+  // copies do not): FP32 kernels of two chunks sharing the SMs run different
+  // variants side by side and thrash the instruction cache, and rescue tiers
+  // queued behind the next chunk's persistent kernels hold back their chunk's
+  // completion, and with it the host's next build, until that chunk's
+  // primary tier ends.
+  cudaEvent_t prev_end = nullptr;
   while (u < units) {
     int64_t u_end = u, bytes = fixed, cells = 0;
     while (u_end < units) {
@@ -1364,10 +1366,10 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     pl.base = (char*)sl.arena.p;
     s.live_bytes = std::max<int64_t>(s.live_bytes, (int64_t)(e->slots[0].arena.bytes + e->slots[1].arena.bytes));
     if ((rc = upload_chunk(&pl, b, &s.h2d_bytes))) return rc;
-    if (prev_primary) VD_CUDA(cudaStreamWaitEvent(pl.stream, prev_primary, 0));
+    if (prev_end) VD_CUDA(cudaStreamWaitEvent(pl.stream, prev_end, 0));
     int launches = 0;
     if ((rc = enqueue_tiers(&pl, &launches))) return rc;
-    prev_primary = pl.ev_mid;
+    prev_end = pl.ev_end;
     s.kernel_launches += launches + (c.n_out > 0 ? 1 : 0);  // the -inf fill of the upload
     const double* dout = (const double*)(pl.base + pl.L.o_out);
     if (c.n_out > 0) {
