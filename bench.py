@@ -6,10 +6,10 @@ Workload (configs[1] shape): 10,000 synthetic regions, 2-16 haplotypes of
 gap-continuation Q10 (vardepth_b200/synthetic.py, seed 1).  A step scores every
 read against every haplotype of its region.
 
-  value    GCUPS of the device-resident plan: the captured CUDA graph of the three
-           kernel tiers (FP32 wavefront, FP32 drift rescue of long reads, FP64 rescue,
-           FP64 32-row strips) on inputs
-           already in HBM, timed with CUDA events on the engine stream, max over ranks.
+  value    GCUPS of the device-resident plan: the captured CUDA graph of the kernel
+           tiers (FP32 wavefront, FP32 drift rescue of long reads, FP64 rescue, FP64
+           32-row strips) on inputs already in HBM, timed with CUDA events on the
+           engine stream, max over ranks.
   e2e      GCUPS through the C-ABI call vd_forward with pinned host buffers: work-list
            build, host->device copies, kernels and the device->host copy of the
            results inside the timed region.
@@ -564,7 +564,7 @@ def main():
                          "unit": "TFLOP/s", "frac": round(achieved / peak.value, 4), "traffic": traffic,
                          "flops_per_cell": FLOPS_PER_CELL, "cells_computed": int(computed),
                          "kernel": "FP32 tier: pairhmm_pair_kernel x2 + pairhmm_kernel<float>"
-                         if args.workload == "config1" else "all three tiers (whole step)",
+                         if args.workload == "config1" else "every tier (whole step)",
                          "primary_ms": round(primary_ms, 3),
                          "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
                          "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},
