@@ -631,11 +631,12 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
     rw.s[r] = make_float2(0.f, 0.f);
   }
 
-  // Shared haplotype prefixes: when hap_share[h] = Q >= 0, haplotype h agrees
-  // with haplotype h-1 of the same region on its first Q bases, so DP columns
-  // 0..Q are the same for both.  The lanes lay their state down in shared
-  // memory (sv) when they finish column Q of h-1 and start h at column Q+1
-  // from it, so the stream carries only columns Q+1..m of h.  Lane 31 also
+  // Shared haplotype prefixes: the item visits its region's haplotypes in
+  // lexicographic order (hap_order); when hap_share = Q >= 0 at position k,
+  // the haplotype there agrees with the one at k-1 on its first Q bases, so
+  // DP columns 0..Q are the same for both.  The lanes lay their state down in
+  // shared memory (sv) when they finish column Q at k-1 and start k at column
+  // Q+1 from it, so the stream carries only columns Q+1..m.  Lane 31 also
   // carries its row sum across.  The row sums are flushed from FP32 into FP64
   // after every column 8r+7 of lane 31 (by column, not by step), so a shared
   // and an unshared pass give the same bits.
@@ -650,7 +651,8 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   auto hap_of = [&](int k) -> int64_t {
     return bv.hap_order != nullptr ? (int64_t)bv.hap_order[w.hap_begin + k] : w.hap_begin + k;
   };
-  int kL = -1, next_reset = 0, S_cur = -1, c0 = 0, save_at = -1;
+  constexpr int kNoSave = INT_MIN;  // no snapshot pending (no stream position, >= -31, matches)
+  int kL = -1, next_reset = 0, S_cur = -1, c0 = 0, save_at = kNoSave;
   const uint8_t* hp = bv.hap_bases;
   float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
   double accA = 0.0, accB = 0.0;
@@ -744,7 +746,7 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
       if (kL >= 0 && lane == kWarp - 1) finalize(kL);
       ++kL;
       S_cur = p;
-      save_at = -1;
+      save_at = kNoSave;
       if (kL < K) {
         const HapMeta& e = ring[kL & (kMetaRing - 1)];
         const int q = e.q;
