@@ -473,3 +473,26 @@ def test_shared_haplotype_prefixes(max_item_columns):
     np.testing.assert_array_equal(plan.fetch(), a)
     plan.close()
     eng.close()
+
+
+def test_drift_tier_error_rich_long_reads():
+    """Long reads at 6% substitution and 2% indel error (configs[4]'s long-read regions) leave
+    a 256-row FP32 strip's range; the drift tier rescores them in FP32 with per-row
+    power-of-two boosts, matching the FP64 oracle, bit-identical under the plain schedule."""
+    rng = np.random.default_rng(404)
+    qf = S._q_standard(rng)
+    regions = []
+    for _ in range(2):
+        hap0 = S._random_hap(rng, 2600)
+        haps = [hap0] + [S._mutate(rng, hap0, 3, 6) for _ in range(2)]
+        reads, quals = S._sim_reads(rng, haps, 4, rng.integers(1000, 2400, 4), 0.06, 0.02, qf)
+        regions.append((haps, reads, quals))
+    w = S._assemble("drift", regions, S.GAP_Q45, S.EXT_Q10, {})
+    eng = native.Engine(0, 4096)
+    batched, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    plain, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED, schedule=native.VD_SCHEDULE_PLAIN)
+    a, st = eng.forward(_packed(w), batched)
+    assert st.rescued_fp32 >= 20 and st.rescued_fp64 + st.rescued_robust <= 2
+    assert_mixed_close(a, _oracle_workload(w))
+    np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], a)
+    eng.close()
