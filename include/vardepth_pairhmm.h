@@ -150,6 +150,18 @@ int vd_forward(vd_engine *engine, const vd_batch *batch, const vd_params *params
                vd_stats *stats);
 int64_t vd_batch_outputs(const vd_batch *batch);
 
+/* The order and shared prefixes in which the two-read kernels stream one
+ * region's haplotypes (no counterpart in the reference: it exposes the rule of
+ * the work-list build, which runs on the host and needs no device).  order[i]
+ * is the haplotype (0 .. n_haps-1) at position i: lexicographic order of the
+ * bases, shorter first on a common prefix, ties in input order.  share[i] = Q
+ * >= 0 when position i starts at DP column Q+1 from the state of column Q
+ * that position i-1's stream laid down or started from (the two agree on
+ * their first Q bases); -1 when it streams from column 0.  Q < its length and
+ * Q >= 32; an empty haplotype shares nothing and ends the chain. */
+int vd_prefix_plan(const unsigned char *hap_bases, const int64_t *hap_off, int64_t n_haps, int32_t *order,
+                   int32_t *share);
+
 /* ---- plans: device-resident batches --------------------------------------
  * vd_plan_create uploads a batch and builds its work list once (ignoring the
  * memory budget); vd_plan_run replays the kernels (captured once into a CUDA

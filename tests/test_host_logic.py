@@ -88,3 +88,73 @@ def test_config1_shape_small():
 def test_workloads_are_seeded():
     a, b = S.config1(n_regions=5), S.config1(n_regions=5)
     assert np.array_equal(a.read_bases, b.read_bases) and np.array_equal(a.hap_bases, b.hap_bases)
+
+
+def _prefix_plan_mirror(haps, min_share=32):
+    """The work-list rule of the two-read kernels restated: lexicographic order (shorter first on a
+    common prefix, ties in input order); a position shares Q bases with the one before it when the
+    snapshot can be laid down while that one streams (Q at or past the column it started from) or
+    is still there (Q equal to its share); Q < its length and >= min_share."""
+    order = sorted(range(len(haps)), key=lambda i: bytes(haps[i]))
+    share, prev = [], -1
+    for k, i in enumerate(order):
+        q = -1
+        if k > 0 and len(haps[i]) > 0 and len(haps[order[k - 1]]) > 0:
+            a, b = haps[order[k - 1]], haps[i]
+            lim = min(len(a), len(b) - 1)
+            l = 0
+            while l < lim and a[l] == b[l]:
+                l += 1
+            if l >= prev + 1:
+                q = l
+            elif prev >= 0 and l >= prev:
+                q = prev
+            if q < min_share:
+                q = -1
+        share.append(q)
+        prev = q
+    return np.array(order, np.int32), np.array(share, np.int32)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_prefix_plan_matches_its_restatement(built_library, seed):
+    """vd_prefix_plan (host only): the order and shared-prefix columns of one region's haplotypes
+    follow the stated rule on families of edited haplotypes, identical copies, prefixes,
+    extensions and empty haplotypes."""
+    from vardepth_b200 import native
+    rng = np.random.default_rng(seed)
+    base = S._random_hap(rng, int(rng.integers(40, 600)))
+    haps = [base]
+    for _ in range(int(rng.integers(1, 20))):
+        kind = rng.integers(0, 6)
+        src = haps[int(rng.integers(0, len(haps)))]
+        if kind == 0:
+            h = src.copy()
+        elif kind == 1:
+            h = src[:int(rng.integers(0, len(src) + 1))]
+        elif kind == 2:
+            h = np.concatenate([src, S._random_hap(rng, int(rng.integers(1, 50)))])
+        elif kind == 3:
+            h = np.empty(0, np.uint8)
+        else:
+            h = S._mutate(rng, src, int(rng.integers(1, 4)), int(rng.integers(0, 8)))
+        haps.append(h)
+    off = np.concatenate([[0], np.cumsum([len(h) for h in haps])]).astype(np.int64)
+    flat = np.concatenate(haps).astype(np.uint8) if off[-1] else np.zeros(1, np.uint8)
+    order, share = native.prefix_plan(flat, off)
+    want_order, want_share = _prefix_plan_mirror(haps)
+    np.testing.assert_array_equal(order, want_order)
+    np.testing.assert_array_equal(share, want_share)
+    # every share is a true common prefix of the two neighbours
+    for k in range(1, len(order)):
+        if share[k] >= 0:
+            a, b = haps[order[k - 1]], haps[order[k]]
+            assert share[k] < len(b) and np.array_equal(a[:share[k]], b[:share[k]])
+
+
+def test_prefix_plan_guards(built_library):
+    from vardepth_b200 import native
+    with pytest.raises(ValueError):
+        native.prefix_plan(np.zeros(4, np.uint8), np.array([0, 3, 2], np.int64))
+    order, share = native.prefix_plan(np.zeros(1, np.uint8), np.array([0], np.int64))
+    assert len(order) == 0 and len(share) == 0

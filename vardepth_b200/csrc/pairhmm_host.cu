@@ -1247,6 +1247,21 @@ int64_t vd_batch_outputs(const vd_batch* b) {
   return batch_outputs(b);
 }
 
+int vd_prefix_plan(const unsigned char* hap_bases, const int64_t* hap_off, int64_t n_haps, int32_t* order,
+                   int32_t* share) {
+  if (n_haps < 0 || (n_haps > 0 && (!hap_off || !order || !share))) return fail(VD_EINVAL, "NULL argument");
+  if (n_haps == 0) return VD_OK;
+  if (n_haps > INT32_MAX || !offsets_ok(hap_off, n_haps))
+    return fail(VD_EINVAL, "haplotype offsets must be non-decreasing (lengths <= 2^28)");
+  if (hap_off[n_haps] > hap_off[0] && !hap_bases) return fail(VD_EINVAL, "haplotype buffer is NULL");
+  vd_batch b{};
+  b.hap_bases = hap_bases;
+  b.hap_off = hap_off;
+  b.n_haps = n_haps;
+  region_order_and_shares(&b, 0, n_haps, 0, order, share);
+  return VD_OK;
+}
+
 int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out, vd_stats* st) {
   const double t0 = now_ms();
   if (!e) return fail(VD_EINVAL, "engine is NULL");

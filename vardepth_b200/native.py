@@ -89,6 +89,8 @@ SIGNATURES = {
     "vd_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams), c_dp,
                                   ctypes.POINTER(VdStats)]),
     "vd_batch_outputs": (c_i64, [ctypes.POINTER(VdBatch)]),
+    "vd_prefix_plan": (ctypes.c_int, [c_u8p, c_i64p, c_i64, ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.POINTER(ctypes.c_int32)]),
     "vd_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdBatch), ctypes.POINTER(VdParams),
                                       ctypes.POINTER(ctypes.c_void_p)]),
     "vd_plan_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VdStats)]),
@@ -208,6 +210,20 @@ class Packed:
         rr = np.diff(self.region_read_off)
         hh = np.diff(self.region_hap_off)
         return int(np.sum(rr * hh))
+
+
+def prefix_plan(hap_bases: np.ndarray, hap_off: np.ndarray):
+    """(order, share) of one region's haplotypes as the two-read kernels stream them
+    (vd_prefix_plan; host only)."""
+    hb = np.ascontiguousarray(hap_bases, dtype=np.uint8)
+    ho = np.ascontiguousarray(hap_off, dtype=np.int64)
+    n = len(ho) - 1
+    order = np.empty(max(n, 0), np.int32)
+    share = np.empty(max(n, 0), np.int32)
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    check(library().vd_prefix_plan(hb.ctypes.data_as(c_u8p), ho.ctypes.data_as(c_i64p), n,
+                                   order.ctypes.data_as(i32p), share.ctypes.data_as(i32p)), "vd_prefix_plan")
+    return order, share
 
 
 def make_params(gap: float, ext: float, anchored: bool, precision: int, quality_offsets=None,
