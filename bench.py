@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """PairHMM GCUPS on B200: the batched FP32-scaled forward against the reference CPU path.
 
-Workload (configs[1] shape): 10,000 synthetic regions, 2-16 haplotypes of
+Workload (batched regions): 10,000 synthetic regions, 2-16 haplotypes of
 100-1,000 bp, lognormal(median 60) reads of 100-250 bp, gap-open Q45 /
 gap-continuation Q10 (vardepth_b200/synthetic.py, seed 1).  A step scores every
 read against every haplotype of its region.
@@ -61,34 +61,36 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
-                    help="run vardepth_b200.autotune on a 2%% region sample first (auto: configs[4] only)")
-    ap.add_argument("--workload", choices=["config1", "config2", "config3", "config4"], default="config1",
-                    help="config1 (default) is the metric's workload; the others print their own line")
+                    help="run vardepth_b200.autotune on a 2%% region sample first (auto: mixed_length_regions only)")
+    ap.add_argument("--workload", default="batched_regions",
+                    choices=["batched_regions", "long_haplotype_stress", "planted_error_model", "mixed_length_regions"],
+                    help="batched_regions (default) is the metric's workload; the others print their own line")
     return ap.parse_args()
 
 
 WORKLOADS = {
-    "config1": "configs[1]: 10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of 100-250 bp, "
-               "gap-open Q45, gap-cont Q10",
-    "config2": "configs[2]: 2000 regions x 4 haps of 1000-5000 bp, 50 reads of 150-300 bp, 20% at 5% error "
-               "and Q2-Q15, gap-open Q45, gap-cont Q10",
-    "config3": "configs[3]: 1000 configs[1]-shaped regions simulated under gap-open Q40, gap-cont Q8, "
-               "bin offsets (+2,-1,0,+3); forward + reverse-wavefront gradient",
-    "config4": "configs[4]: 200000 regions, 2-32 haps of lognormal(400) 80-8000 bp, lognormal(40) reads of "
-               "150 bp, 2% of regions with 1-10 kb reads at 8% error, gap-open Q45, gap-cont Q10",
+    "batched_regions": "10000 regions, 2-16 haps of 100-1000 bp, lognormal(60) reads of 100-250 bp, "
+                       "gap-open Q45, gap-cont Q10",
+    "long_haplotype_stress": "2000 regions x 4 haps of 1000-5000 bp, 50 reads of 150-300 bp, 20% at 5% "
+                             "error and Q2-Q15, gap-open Q45, gap-cont Q10",
+    "planted_error_model": "1000 batched-regions-shaped regions simulated under gap-open Q40, gap-cont Q8, "
+                           "bin offsets (+2,-1,0,+3); forward + reverse-wavefront gradient",
+    "mixed_length_regions": "200000 regions, 2-32 haps of lognormal(400) 80-8000 bp, lognormal(40) reads of "
+                            "150 bp, 2% of regions with 1-10 kb reads at 8% error, gap-open Q45, gap-cont Q10",
 }
-DEFAULT_REGIONS = {"config1": 10_000, "config2": 2_000, "config3": 1_000, "config4": 200_000}
+DEFAULT_REGIONS = {"batched_regions": 10_000, "long_haplotype_stress": 2_000, "planted_error_model": 1_000,
+                   "mixed_length_regions": 200_000}
 
 
 def make_workload(name, regions):
     from vardepth_b200 import synthetic
-    if name == "config1":
-        return synthetic.config1(n_regions=regions)
-    if name == "config2":
-        return synthetic.config2(n_regions=regions)
-    if name == "config3":
-        return synthetic.config3(n_regions=regions)
-    return synthetic.config4(n_regions=regions, workers=0)
+    if name == "batched_regions":
+        return synthetic.batched_regions(n_regions=regions)
+    if name == "long_haplotype_stress":
+        return synthetic.long_haplotype_stress(n_regions=regions)
+    if name == "planted_error_model":
+        return synthetic.planted_error_model(n_regions=regions)
+    return synthetic.mixed_length_regions(n_regions=regions, workers=0)
 
 
 # ---- CPU reference (oracle/_ref, the reference's own wide.cpp) -----------------------
@@ -256,11 +258,11 @@ def reference_arm(args):
 
 
 def gradient_arm(args, local):
-    """configs[3]: forward + reverse-wavefront gradient, checkpoint modes, accuracy and the fit."""
+    """forward + reverse-wavefront gradient, checkpoint modes, accuracy and the fit."""
     import torch
     from vardepth_b200 import autograd as AG
     from vardepth_b200 import native
-    w = make_workload("config3", args.regions)
+    w = make_workload("planted_error_model", args.regions)
     packed = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
                            region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
     engine = native.Engine(local, 65536)
@@ -310,10 +312,11 @@ def gradient_arm(args, local):
     theta = AG.fit_error_model(batch, w.region_read_off, w.region_hap_off, theta0, history=hist)
     fit_s = time.perf_counter() - t0
     planted = np.array(w.meta["planted"])
-    line = {"metric": "PairHMM forward+gradient GCUPS on 1 B200 (configs[3])", "value": modes["sqrt"]["gcups"],
+    line = {"metric": "PairHMM forward+gradient GCUPS on 1 B200 (planted-error-model workload)",
+            "value": modes["sqrt"]["gcups"],
             "unit": "GCUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": modes["sqrt"]["kernel_ms"], "higher_is_better": True, "dtype": "fp32",
-            "data": "synthetic", "config": {"workload": WORKLOADS["config3"], "regions": args.regions,
+            "data": "synthetic", "config": {"workload": WORKLOADS["planted_error_model"], "regions": args.regions,
                                             "pairs": w.pairs(), "cells": cells, "seed": w.meta.get("seed")},
             "checkpointing": modes, "forward_gcups": round(cells / (fw_ms / args.steps) / 1e6, 3),
             "gradient_check": check,
@@ -346,7 +349,7 @@ def main():
     torch.cuda.set_device(local)
 
     from vardepth_b200 import native
-    if args.workload == "config3":
+    if args.workload == "planted_error_model":
         gradient_arm(args, local)
         return
     w = make_workload(args.workload, args.regions)
@@ -386,7 +389,7 @@ def main():
 
     # ---- autotuner: work-list choices timed on a region sample, kept on the engine ----
     tuned = None
-    if args.autotune == "on" or (args.autotune == "auto" and args.workload == "config4"):
+    if args.autotune == "on" or (args.autotune == "auto" and args.workload == "mixed_length_regions"):
         from vardepth_b200 import autotune
         sub = w.subset(autotune.sample_regions(w.region_read_off, w.region_hap_off, fraction=0.02))
         sp = native.Packed(sub.read_bases, sub.read_quals, sub.read_off, sub.hap_bases, sub.hap_off,
@@ -534,19 +537,19 @@ def main():
                "kind": "reference", "sample": res["sample"]}
 
     primary_ms = allmax(primary_ms) / args.steps
-    # the primary tier holds all but ~0.5% of the work; elsewhere the
-    # FP64 tiers can hold a real share, so the whole step is the denominator
-    roof_ms = primary_ms if args.workload == "config1" else step_ms
+    # batched regions: the primary tier holds all but ~0.5% of the work; elsewhere
+    # the rescue tiers can hold a real share, so the whole step is the denominator
+    roof_ms = primary_ms if args.workload == "batched_regions" else step_ms
     # the FMA pipe only sees the cells it computes: columns a haplotype shares
     # with the previous one of its region are counted in value, not here
     computed = cells - shared
     achieved = computed * FLOPS_PER_CELL / (roof_ms / 1e3) / 1e12
     traffic = None
     tf = ROOT / "profiles" / "pairhmm_f32_traffic.json"
-    if tf.exists() and args.workload == "config1":
+    if tf.exists() and args.workload == "batched_regions":
         try:
             t = json.loads(tf.read_text())
-            traffic = t.get("bytes_per_launch_full_config1")
+            traffic = t.get("bytes_per_launch_full_batched_regions")
         except (OSError, ValueError):
             traffic = None
     if rank == 0:
@@ -564,7 +567,7 @@ def main():
                          "unit": "TFLOP/s", "frac": round(achieved / peak.value, 4), "traffic": traffic,
                          "flops_per_cell": FLOPS_PER_CELL, "cells_computed": int(computed),
                          "kernel": "FP32 tier: pairhmm_pair_kernel x2 + pairhmm_kernel<float>"
-                         if args.workload == "config1" else "every tier (whole step)",
+                         if args.workload == "batched_regions" else "every tier (whole step)",
                          "primary_ms": round(primary_ms, 3),
                          "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
                          "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},

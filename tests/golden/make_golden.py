@@ -13,11 +13,11 @@ used).  Shapes and seeds are those of the reference's tests:
   catalog_seed7713.npz tests/test_cpu_catalog.py:22-31  (anchored_pairhmm values)
   edge_cases.npz       tests/test_accelerator.py:21-40 shapes plus N bases, Q0/Q1/Q255,
                        1x1 and empty pairs
-  config0_q45.npz      configs[0] workload (seed 0) at gap 10^-4.5 / ext 0.1 through
+  single_region_q45.npz      the single-region workload workload (seed 0) at gap 10^-4.5 / ext 0.1 through
                        wide.cpp read_haplotype_batch_mode
-  config0_q30.npz      the same reads at the production 0.001 / 0.1 through
+  single_region_q30.npz      the same reads at the production 0.001 / 0.1 through
                        cpu_batch.pairs (trie_many, the production CPU path)
-  genotypes_seed4242.npz  12 configs[1]-shaped regions: ln L from wide.cpp
+  genotypes_seed4242.npz  12 batched-regions-shaped regions: ln L from wide.cpp
                        read_haplotype_batch_mode, then per region molecule_rows.normalized_rows
                        with seeded mapping qualities, triangular._diploid_likelihood_numpy (no
                        prior) and mixture_cpu.general (mixture_general.cpp) at priors 0 and 0.001
@@ -178,8 +178,8 @@ def main():
     out["edge_cases"] = dict(pack(pairs), semiglobal=sg, anchored=an, prepared=prepared,
                              n_prepared=np.int64(len(prepared)), gap=0.001, ext=0.1)
 
-    # configs[0] at the benchmark's Q45/Q10 and at the production 0.001/0.1
-    w = synthetic.config0()
+    # the single-region workload at the benchmark's Q45/Q10 and at the production 0.001/0.1
+    w = synthetic.single_region()
     seqs, qls = [], []
     for r in range(len(w.read_off) - 1):
         a, b = w.read_off[r], w.read_off[r + 1]
@@ -191,9 +191,9 @@ def main():
     q45 = np.stack([O.ref_batch_mode(s, q, haps, gap=w.gap, ext=w.ext) for s, q in zip(seqs, qls)])
     base = dict(read_bases=w.read_bases, read_quals=w.read_quals, read_off=w.read_off, hap_bases=w.hap_bases,
                 hap_off=w.hap_off, region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
-    out["config0_q45"] = dict(base, semiglobal=q45.ravel(), gap=w.gap, ext=w.ext)
+    out["single_region_q45"] = dict(base, semiglobal=q45.ravel(), gap=w.gap, ext=w.ext)
     prod = cpu_batch.many(seqs, qls, haps, mode=0)
-    out["config0_q30"] = dict(base, semiglobal=np.asarray(prod).ravel(), gap=0.001, ext=0.1)
+    out["single_region_q30"] = dict(base, semiglobal=np.asarray(prod).ravel(), gap=0.001, ext=0.1)
 
     # region post-processing (molecule_rows.py, triangular.py, mixture_general.cpp)
     blocks = types.ModuleType("blocks")
@@ -203,7 +203,7 @@ def main():
     rows = load_source("molecule_rows", REFERENCE / "molecule_rows.py")
     tri = load_source("triangular", REFERENCE / "triangular.py")
     mix = load_source("mixture_cpu", REFERENCE / "mixture_cpu.py")
-    w = synthetic.config1(seed=4242, n_regions=12)
+    w = synthetic.batched_regions(seed=4242, n_regions=12)
     mq = np.random.default_rng(4242).choice([0, 3, 20, 37, 60, 255], size=len(w.read_off) - 1).astype(np.uint8)
     lns, vals, cert, gl_none, gl_p0, gl_p001 = [], [], [], [], [], []
     for g in range(w.n_regions):

@@ -61,7 +61,7 @@ def test_matches_reference_postprocessing(engine, prior, key):
 
 
 def test_mixed_precision_calls_and_optional_outputs(engine):
-    w = S.config1(n_regions=40, seed=17)
+    w = S.batched_regions(n_regions=40, seed=17)
     pk = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
                        region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
     params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
@@ -87,7 +87,7 @@ def test_mixed_precision_calls_and_optional_outputs(engine):
 def test_near_tie_guard_rescores_tied_regions_in_fp64(engine):
     """partial_anchor.py:120-133 as a device flag: a region whose haplotypes are all identical ties
     every genotype and is rescored in FP64; a region with a clear call keeps its mixed-precision result."""
-    w = S.config1(n_regions=6, seed=21)
+    w = S.batched_regions(n_regions=6, seed=21)
     # every haplotype of region 0 is a copy of its first: all its genotypes tie
     haps = [w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]] for h in range(len(w.hap_off) - 1)]
     h0 = w.region_hap_off[0]

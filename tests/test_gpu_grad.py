@@ -51,7 +51,7 @@ def _fb(engine, packed, theta, precision=native.VD_PRECISION_MIXED, checkpoint=n
 
 @pytest.mark.parametrize("theta", [THETA, np.array([40.0, 8.0, 2.0, -1.0, 0.0, 3.0])])
 def test_jacobian_matches_expected_count_oracle(engine, theta):
-    w = S.config1(n_regions=6)
+    w = S.batched_regions(n_regions=6)
     lo, jo = _oracle(w, theta)
     ln, jac, st = _fb(engine, _packed(w), theta)
     assert st.failed_pairs == 0 and st.pairs == w.pairs()
@@ -68,7 +68,7 @@ def test_jacobian_matches_expected_count_oracle(engine, theta):
 
 
 def test_ln_matches_forward(engine):
-    w = S.config1(n_regions=20)
+    w = S.batched_regions(n_regions=20)
     params, _keep = AG.params_from_theta(THETA)
     fw, _ = engine.forward(_packed(w), params)
     ln, _, _ = _fb(engine, _packed(w), THETA)
@@ -77,7 +77,7 @@ def test_ln_matches_forward(engine):
 
 @pytest.mark.parametrize("precision", [native.VD_PRECISION_MIXED, native.VD_PRECISION_FLOAT64])
 def test_sqrt_checkpointing_equals_storing_every_antidiagonal(engine, precision):
-    w = S.config1(n_regions=12)
+    w = S.batched_regions(n_regions=12)
     a = _fb(engine, _packed(w), THETA, precision, native.VD_CHECKPOINT_SQRT)
     b = _fb(engine, _packed(w), THETA, precision, native.VD_CHECKPOINT_ALL)
     np.testing.assert_array_equal(a[0], b[0])
@@ -86,7 +86,7 @@ def test_sqrt_checkpointing_equals_storing_every_antidiagonal(engine, precision)
 
 
 def test_central_differences(engine):
-    w = S.config0()
+    w = S.single_region()
     pr, ph = w.explicit_pairs()
     sel = np.arange(0, len(pr), 16)
     pk = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off, pair_read=pr[sel],
@@ -200,7 +200,7 @@ def test_empty_inputs_and_argument_errors(engine):
 
 
 def test_autograd_backward_is_grad_output_times_jacobian(engine):
-    w = S.config1(n_regions=4)
+    w = S.batched_regions(n_regions=4)
     batch = AG.Batch(engine, _packed(w))
     theta = torch.tensor(THETA, dtype=torch.float32, requires_grad=True)
     ln = AG.loglik(theta, batch)
@@ -215,9 +215,9 @@ def test_autograd_backward_is_grad_output_times_jacobian(engine):
 
 
 def test_fit_recovers_planted_parameters(engine):
-    """configs[3] shape at 300 regions: reads simulated at gap-open Q40, gap-continuation Q8 and
+    """the planted-error-model workload shape at 300 regions: reads simulated at gap-open Q40, gap-continuation Q8 and
     offsets (+2, -1, 0, +3); L-BFGS from Q45 / Q10 / zeros lands within 1 Phred of each."""
-    w = S.config3(n_regions=300)
+    w = S.planted_error_model(n_regions=300)
     batch = AG.Batch(engine, _packed(w))
     hist = []
     theta = AG.fit_error_model(batch, w.region_read_off, w.region_hap_off, [45.0, 10.0, 0, 0, 0, 0], history=hist)

@@ -96,7 +96,7 @@ def test_edge_cases(mixed, fp64, anchored):
     assert np.isneginf(empty).all()
 
 
-@pytest.mark.parametrize("name", ["config0_q45", "config0_q30"])
+@pytest.mark.parametrize("name", ["single_region_q45", "single_region_q30"])
 def test_config0_against_reference(mixed, name):
     d = golden(name)
     packed = native.Packed(d["read_bases"], d["read_quals"], d["read_off"], d["hap_bases"], d["hap_off"],
@@ -135,13 +135,13 @@ def _argmax_agree(w, got, want):
 
 
 def test_config1_sample_against_oracle(mixed):
-    w = S.config1(n_regions=24)
+    w = S.batched_regions(n_regions=24)
     got = _with(mixed, w.gap, w.ext).score_packed(_packed(w))
     want = _oracle_workload(w)
     err = assert_mixed_close(got, want)
     agree, total = _argmax_agree(w, got, want)
     assert agree == total
-    print(f"config1 sample: pairs {len(got)} max|dlog10| {err.max():.2e} "
+    print(f"batched_regions sample: pairs {len(got)} max|dlog10| {err.max():.2e} "
           f"p99 {np.quantile(err, .99):.2e} rescued {mixed.last['float64_fallback_pairs']}")
 
 
@@ -180,13 +180,13 @@ def test_anchored_refinement_windows(mixed, fp64):
 
 
 def test_config2_precision_stress(mixed):
-    w = S.config2(n_regions=6)
+    w = S.long_haplotype_stress(n_regions=6)
     got = _with(mixed, w.gap, w.ext).score_packed(_packed(w))
     want = _oracle_workload(w)
     err = assert_mixed_close(got, want)
     agree, total = _argmax_agree(w, got, want)
     assert agree == total
-    print(f"config2 sample: pairs {len(got)} max|dlog10| {err.max():.2e} rescued "
+    print(f"long_haplotype_stress sample: pairs {len(got)} max|dlog10| {err.max():.2e} rescued "
           f"{mixed.last['float64_fallback_pairs']}/{len(got)}")
 
 
@@ -209,7 +209,7 @@ def test_long_reads_strip_mined(mixed, fp64, anchored):
 
 
 def test_pairs_regions_and_chunking_agree():
-    w = S.config1(n_regions=200)
+    w = S.batched_regions(n_regions=200)
     eng = CudaPairHMM(memory_mb=4096, gap=w.gap, ext=w.ext)
     regions = eng.score_packed(_packed(w))
     pr, ph = w.explicit_pairs()
@@ -228,7 +228,7 @@ def test_pairs_regions_and_chunking_agree():
 def test_pipelined_chunks_agree():
     """vd_forward's pipelined chunks (the first a quarter of the others, each chunk's
     primary tier ordered after the previous one's) give the single-chunk results bit for bit."""
-    w = S.config1(n_regions=300)
+    w = S.batched_regions(n_regions=300)
     eng = native.Engine(0, 8192)
     params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
     eng.set_tuning(pipeline_gcells=1_000_000)
@@ -245,7 +245,7 @@ def test_pipelined_chunks_agree():
 
 
 def test_plan_graph_replay_is_deterministic():
-    w = S.config1(n_regions=16)
+    w = S.batched_regions(n_regions=16)
     eng = native.Engine(0, 4096)
     params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
     plan = eng.plan(_packed(w), params)
@@ -265,7 +265,7 @@ def test_plan_graph_replay_is_deterministic():
 def test_plain_schedule_gives_identical_results(anchored, precision):
     """VD_SCHEDULE_PLAIN (one pair per item, fixed 8 rows per lane, input order) runs the same
     arithmetic as the batched schedule, so every pair agrees bit for bit; long reads included."""
-    w = S.config1(n_regions=40)
+    w = S.batched_regions(n_regions=40)
     eng = native.Engine(0, 4096)
     batched, _ = native.make_params(w.gap, w.ext, anchored, precision)
     plain, _ = native.make_params(w.gap, w.ext, anchored, precision, schedule=native.VD_SCHEDULE_PLAIN)
@@ -302,8 +302,8 @@ def test_reference_shaped_entry_points():
                                   8, out.ctypes.data_as(native.c_dp))
         assert rc == 0, native.last_error()
         assert_mixed_close(out, d[key])
-    # trie_many: reads x haplotypes of config0 at the production constants
-    g = golden("config0_q30")
+    # trie_many: reads x haplotypes of single_region at the production constants
+    g = golden("single_region_q30")
     nr, nh = len(g["read_off"]) - 1, len(g["hap_off"]) - 1
     rb = [bytes(g["read_bases"][g["read_off"][i]:g["read_off"][i + 1]]) for i in range(nr)]
     qb = [bytes(g["read_quals"][g["read_off"][i]:g["read_off"][i + 1]]) for i in range(nr)]
@@ -317,7 +317,7 @@ def test_reference_shaped_entry_points():
     assert rc == 0 and cells.value == sum(map(len, rb)) * sum(map(len, hb))
     assert_mixed_close(out, g["semiglobal"])
     # read_haplotype_batch_mode with the benchmark's gap/ext
-    q45 = golden("config0_q45")
+    q45 = golden("single_region_q45")
     s0 = rb[0]
     q0 = (ctypes.c_ubyte * len(qb[0]))(*qb[0])
     out2 = np.empty(nh)
@@ -390,7 +390,7 @@ def test_long_read_strip_heights(rows, anchored):
 
 def test_autotune_on_a_sample():
     from vardepth_b200 import autotune
-    w = S.config4(n_regions=120, workers=1)
+    w = S.mixed_length_regions(n_regions=120, workers=1)
     sub = w.subset(autotune.sample_regions(w.region_read_off, w.region_hap_off, fraction=0.5, min_regions=40))
     eng = native.Engine(0, 8192)
     params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
@@ -407,7 +407,7 @@ def test_autotune_on_a_sample():
 def test_region_shards_score_like_the_whole_batch():
     """Each rank's shard (LPT by cells) scored on its own gives the whole batch's values."""
     from vardepth_b200 import shard
-    w = S.config1(n_regions=50, seed=9)
+    w = S.batched_regions(n_regions=50, seed=9)
     pk = _packed(w)
     eng = native.Engine(0, 4096)
     params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
@@ -476,7 +476,7 @@ def test_shared_haplotype_prefixes(max_item_columns):
 
 
 def test_drift_tier_error_rich_long_reads():
-    """Long reads at 6% substitution and 2% indel error (configs[4]'s long-read regions) leave
+    """Long reads at 6% substitution and 2% indel error (the mixed-length workload's long-read regions) leave
     a 256-row FP32 strip's range; the drift tier rescores them in FP32 with per-row
     power-of-two boosts, matching the FP64 oracle, bit-identical under the plain schedule."""
     rng = np.random.default_rng(404)

@@ -1,6 +1,6 @@
 """The gradient checker itself, on the CPU: the long-double expected-count gradient of the
 oracle against central finite differences of the FP64 forward restatement (h = 1e-3 on
-the Phred-scale parameters), and the configs[3] simulator's shape."""
+the Phred-scale parameters), and the the planted-error-model workload simulator's shape."""
 import numpy as np
 import pytest
 
@@ -23,7 +23,7 @@ def _pairs(w, k):
 def test_expected_count_gradient_matches_finite_differences(anchored, theta):
     theta = np.array(theta)
     g, x = O.phred_to_prob(theta[0]), O.phred_to_prob(theta[1])
-    for read, qual, hap in _pairs(S.config0(), 6):
+    for read, qual, hap in _pairs(S.single_region(), 6):
         ln, jac = O.grad(read, qual, hap, g, x, anchored, theta[2:])
         fd = O.fd_grad(read, qual, hap, theta, anchored=anchored)
         assert np.isclose(ln, O.forward(read, qual, hap, g, x, anchored, O.SEMIGLOBAL_ROW_DIVIDE, offsets=theta[2:]),
@@ -45,7 +45,7 @@ def test_low_quality_bases_and_two_sided_emissions():
 
 
 def test_batch_gradient_matches_single_pairs():
-    w = S.config0()
+    w = S.single_region()
     pr, ph = w.explicit_pairs()
     pr, ph = pr[:10], ph[:10]
     theta = np.array([42.0, 9.0, 1.0, -0.5, 0.25, 2.0])
@@ -59,14 +59,14 @@ def test_batch_gradient_matches_single_pairs():
 
 
 def test_planted_simulation_shape():
-    w = S.config3(n_regions=20)
+    w = S.planted_error_model(n_regions=20)
     assert w.meta["planted"] == [40.0, 8.0, 2.0, -1.0, 0.0, 3.0]
     n = np.diff(w.read_off)
     assert n.min() >= 1 and n.max() <= 250
     assert set(np.unique(w.read_quals)) <= {10, 20, 30, 40}
     assert w.n_regions == 20
     # reproducible from the seed
-    w2 = S.config3(n_regions=20)
+    w2 = S.planted_error_model(n_regions=20)
     np.testing.assert_array_equal(w.read_bases, w2.read_bases)
 
 

@@ -63,7 +63,7 @@ def test_quality_objects_are_validated_once_and_kept():
 
 
 def test_config0_shape():
-    w = S.config0()
+    w = S.single_region()
     assert w.n_regions == 1 and len(w.read_off) - 1 == 64 and list(w.hap_lengths()) == [300, 297]
     assert set(np.unique(w.read_quals)) <= {10, 20, 30, 40}
     assert w.pairs() == 128 and w.cells() == 64 * 150 * 597
@@ -71,7 +71,7 @@ def test_config0_shape():
 
 
 def test_config1_shape_small():
-    w = S.config1(n_regions=40)
+    w = S.batched_regions(n_regions=40)
     nh = np.diff(w.region_hap_off)
     nr = np.diff(w.region_read_off)
     assert nh.min() >= 2 and nh.max() <= 16 and nr.min() >= 10 and nr.max() <= 500
@@ -86,7 +86,7 @@ def test_config1_shape_small():
 
 
 def test_workloads_are_seeded():
-    a, b = S.config1(n_regions=5), S.config1(n_regions=5)
+    a, b = S.batched_regions(n_regions=5), S.batched_regions(n_regions=5)
     assert np.array_equal(a.read_bases, b.read_bases) and np.array_equal(a.hap_bases, b.hap_bases)
 
 

@@ -52,8 +52,8 @@ def _region_pairs(d):
     return O.region_pairs(d["region_read_off"], d["region_hap_off"])
 
 
-def test_restatement_config0_q45_and_production():
-    for name in ("config0_q45", "config0_q30"):
+def test_restatement_single_region_q45_and_production():
+    for name in ("single_region_q45", "single_region_q30"):
         d = golden(name)
         pr, ph = _region_pairs(d)
         got = O.forward_pairs(d["read_bases"], d["read_quals"], d["read_off"], d["hap_bases"], d["hap_off"], pr, ph,

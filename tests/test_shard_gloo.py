@@ -15,7 +15,7 @@ from vardepth_b200 import synthetic as S
 
 
 def _workload():
-    w = S.config1(n_regions=30, seed=5)
+    w = S.batched_regions(n_regions=30, seed=5)
     return w, native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
                             region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
 

@@ -980,7 +980,7 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
 // each entry in the two-sided emission form its boosted match factors need,
 // on its own kernel so the strip driver's state does not crowd the primary
 // kernel's registers (launched with 4 blocks per SM, 128 registers: 7% faster
-// on configs[4]'s long reads than 3 blocks at 162 registers without spills).
+// on the mixed-length workload's long reads than 3 blocks at 162 registers without spills).
 // Entries whose rows per lane have no strip-mined variant go on to FP64
 // unchanged.
 template <int kBlocks>

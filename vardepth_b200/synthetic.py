@@ -3,20 +3,20 @@
 The reference benchmarks this stage on no public dataset, so reads and
 haplotypes are simulated (numpy.random.default_rng(seed), seeds 0-4):
 
-* ``config0``  one region: hap0 300 bp uniform ACGT, hap1 = hap0 with an SNV at
+* ``single_region``  one region: hap0 300 bp uniform ACGT, hap1 = hap0 with an SNV at
   150 and a 3 bp deletion at 220; 64 reads of 150 bp, start uniform, source
   haplotype 50/50, 1% substitution and 0.1% 1-bp indel error, qualities i.i.d.
   from Q{10,20,30,40} with probabilities {.05,.15,.5,.3}; gap-open Q45,
   gap-continuation Q10.
-* ``config1``  10,000 regions; haplotypes per region U{2..16}, first haplotype
+* ``batched_regions``  10,000 regions; haplotypes per region U{2..16}, first haplotype
   U{100..1000} bp, every other one the first with 1-4 SNVs and one 1-10 bp
   indel; reads per region round(lognormal(ln 60, 1.0)) clipped to 10..500,
   read length U{100..250} (at most the source haplotype's length); errors and
-  qualities as config0.
-* ``config2``  2,000 regions x 4 haplotypes of U{1000..5000} bp; 50 reads of
+  qualities as single_region.
+* ``long_haplotype_stress``  2,000 regions x 4 haplotypes of U{1000..5000} bp; 50 reads of
   U{150..300} bp per region; 20% of the reads carry 5% substitution error with
   qualities U{2..15}.
-* ``config3``  1,000 regions shaped as config1, with reads drawn from the
+* ``planted_error_model``  1,000 regions shaped as batched_regions, with reads drawn from the
   PairHMM's own generative model under planted parameters: gap-open Q40,
   gap-continuation Q8, and true base errors 10^(-(q + o_bin)/10) for the
   reported quality q with bin offsets (+2, -1, 0, +3) (bins q<15, q<25,
@@ -24,7 +24,7 @@ haplotypes are simulated (numpy.random.default_rng(seed), seeds 0-4):
   uniform column of its source haplotype; every M state moves to M, I or D
   with 1-2g, g, g; I and D extend with x; M emits the haplotype base (a
   uniform other base with probability e), I a uniform base, D nothing.
-* ``config4``  200,000 regions; haplotype length lognormal (median 400, sigma
+* ``mixed_length_regions``  200,000 regions; haplotype length lognormal (median 400, sigma
   0.6) clipped to 80..8000, U{2..32} haplotypes; reads lognormal (median 40,
   sigma 1.0) clipped to 4..2000 of 150 bp; 2% of regions instead carry
   U{2..8} reads of 1-10 kb at 8% error (6% substitution, 2% 1-bp indel) against
@@ -224,17 +224,17 @@ def _assemble(name, regions, gap, ext, meta) -> Workload:
                     False, meta)
 
 
-def config0(seed: int = 0, gap: float = GAP_Q45, ext: float = EXT_Q10) -> Workload:
+def single_region(seed: int = 0, gap: float = GAP_Q45, ext: float = EXT_Q10) -> Workload:
     rng = np.random.default_rng(seed)
     hap0 = _random_hap(rng, 300)
     hap1 = hap0.copy()
     hap1[150] = ALPHABET[ALPHABET != hap0[150]][rng.integers(0, 3)]
     hap1 = np.concatenate([hap1[:220], hap1[223:]])
     reads, quals = _sim_reads(rng, [hap0, hap1], 64, np.full(64, 150), 0.01, 0.001, _q_standard(rng))
-    return _assemble("config0", [([hap0, hap1], reads, quals)], gap, ext, {"seed": seed})
+    return _assemble("single_region", [([hap0, hap1], reads, quals)], gap, ext, {"seed": seed})
 
 
-def config1(seed: int = 1, n_regions: int = 10_000, gap: float = GAP_Q45, ext: float = EXT_Q10,
+def batched_regions(seed: int = 1, n_regions: int = 10_000, gap: float = GAP_Q45, ext: float = EXT_Q10,
             sigma: float = 1.0) -> Workload:
     rng = np.random.default_rng(seed)
     qf = _q_standard(rng)
@@ -246,10 +246,10 @@ def config1(seed: int = 1, n_regions: int = 10_000, gap: float = GAP_Q45, ext: f
         nr = int(np.clip(round(rng.lognormal(np.log(60), sigma)), 10, 500))
         reads, quals = _sim_reads(rng, haps, nr, rng.integers(100, 251, nr), 0.01, 0.001, qf)
         regions.append((haps, reads, quals))
-    return _assemble("config1", regions, gap, ext, {"seed": seed, "sigma": sigma, "regions": n_regions})
+    return _assemble("batched_regions", regions, gap, ext, {"seed": seed, "sigma": sigma, "regions": n_regions})
 
 
-def config2(seed: int = 2, n_regions: int = 2_000, gap: float = GAP_Q45, ext: float = EXT_Q10) -> Workload:
+def long_haplotype_stress(seed: int = 2, n_regions: int = 2_000, gap: float = GAP_Q45, ext: float = EXT_Q10) -> Workload:
     rng = np.random.default_rng(seed)
     qf = _q_standard(rng)
     low_q = lambda n: rng.integers(2, 16, n).astype(np.uint8)
@@ -262,7 +262,7 @@ def config2(seed: int = 2, n_regions: int = 2_000, gap: float = GAP_Q45, ext: fl
         good_r, good_q = _sim_reads(rng, haps, int((~bad).sum()), lengths[~bad], 0.01, 0.001, qf)
         bad_r, bad_q = _sim_reads(rng, haps, int(bad.sum()), lengths[bad], 0.05, 0.0, low_q)
         regions.append((haps, good_r + bad_r, good_q + bad_q))
-    return _assemble("config2", regions, gap, ext, {"seed": seed, "regions": n_regions})
+    return _assemble("long_haplotype_stress", regions, gap, ext, {"seed": seed, "regions": n_regions})
 
 
 PLANTED_Q_GAP = 40.0
@@ -333,9 +333,9 @@ def _sim_hmm_reads(rng, haps, n_reads, lengths, gap, ext, offsets, quals_fn):
     return reads, quals
 
 
-def config3(seed: int = 3, n_regions: int = 1_000, q_gap: float = PLANTED_Q_GAP, q_ext: float = PLANTED_Q_EXT,
+def planted_error_model(seed: int = 3, n_regions: int = 1_000, q_gap: float = PLANTED_Q_GAP, q_ext: float = PLANTED_Q_EXT,
             offsets=PLANTED_OFFSETS, sigma: float = 1.0) -> Workload:
-    """config1-shaped regions whose reads follow the model under planted parameters."""
+    """batched_regions-shaped regions whose reads follow the model under planted parameters."""
     rng = np.random.default_rng(seed)
     qf = _q_standard(rng)
     gap, ext = 10.0 ** (-q_gap / 10.0), 10.0 ** (-q_ext / 10.0)
@@ -347,7 +347,7 @@ def config3(seed: int = 3, n_regions: int = 1_000, q_gap: float = PLANTED_Q_GAP,
         nr = int(np.clip(round(rng.lognormal(np.log(60), sigma)), 10, 500))
         reads, quals = _sim_hmm_reads(rng, haps, nr, rng.integers(100, 251, nr), gap, ext, offsets, qf)
         regions.append((haps, reads, quals))
-    return _assemble("config3", regions, GAP_Q45, EXT_Q10,
+    return _assemble("planted_error_model", regions, GAP_Q45, EXT_Q10,
                      {"seed": seed, "regions": n_regions, "planted": [q_gap, q_ext, *offsets]})
 
 
@@ -370,37 +370,37 @@ def _concat(parts, name, gap, ext, meta) -> Workload:
                     join_off("region_read_off"), join_off("region_hap_off"), gap, ext, False, meta)
 
 
-_CONFIG4_BLOCK = 2_000
+_MIXED_BLOCK = 2_000
 
 
-def _config4_block(args) -> Workload:
+def _mixed_block(args) -> Workload:
     seed, block, count, gap, ext = args
     rng = np.random.default_rng([seed, block])
-    return _config4_regions(rng, count, gap, ext)
+    return _mixed_regions(rng, count, gap, ext)
 
 
-def config4(seed: int = 4, n_regions: int = 200_000, gap: float = GAP_Q45, ext: float = EXT_Q10,
+def mixed_length_regions(seed: int = 4, n_regions: int = 200_000, gap: float = GAP_Q45, ext: float = EXT_Q10,
             workers: int = 1) -> Workload:
     """Regions are drawn in blocks of 2,000, block b from default_rng([seed, b]), so the
     blocks can be generated on several host processes (workers > 1; 0 = every core).  The
     processes are spawned, so a script that asks for workers != 1 must call this under
     ``if __name__ == "__main__":``."""
     import os
-    blocks = [(seed, b, min(_CONFIG4_BLOCK, n_regions - b * _CONFIG4_BLOCK), gap, ext)
-              for b in range((n_regions + _CONFIG4_BLOCK - 1) // _CONFIG4_BLOCK)]
+    blocks = [(seed, b, min(_MIXED_BLOCK, n_regions - b * _MIXED_BLOCK), gap, ext)
+              for b in range((n_regions + _MIXED_BLOCK - 1) // _MIXED_BLOCK)]
     if workers == 0:
         workers = min(len(blocks), len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else 1)
     if workers > 1 and len(blocks) > 1:
         import multiprocessing as mp
         # spawn: a forked child of a process that holds a CUDA context can hang
         with mp.get_context("spawn").Pool(workers) as pool:
-            parts = pool.map(_config4_block, blocks)
+            parts = pool.map(_mixed_block, blocks)
     else:
-        parts = [_config4_block(b) for b in blocks]
-    return _concat(parts, "config4", gap, ext, {"seed": seed, "regions": n_regions})
+        parts = [_mixed_block(b) for b in blocks]
+    return _concat(parts, "mixed_length_regions", gap, ext, {"seed": seed, "regions": n_regions})
 
 
-def _config4_regions(rng, n_regions: int, gap: float, ext: float) -> Workload:
+def _mixed_regions(rng, n_regions: int, gap: float, ext: float) -> Workload:
     qf = _q_standard(rng)
     regions = []
     for _ in range(n_regions):
@@ -421,7 +421,7 @@ def _config4_regions(rng, n_regions: int, gap: float, ext: float) -> Workload:
             nr = int(np.clip(round(rng.lognormal(np.log(40), 1.0)), 4, 2000))
             reads, quals = _sim_reads(rng, haps, nr, np.full(nr, 150), 0.01, 0.001, qf)
         regions.append((haps, reads, quals))
-    return _assemble("config4", regions, gap, ext, {})
+    return _assemble("mixed_length_regions", regions, gap, ext, {})
 
 
 def random_pairs(seed: int, shapes, copies: int, qlo: int = 0, qhi: int = 61, alphabet="ACGT"):
