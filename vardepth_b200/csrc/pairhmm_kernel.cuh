@@ -149,8 +149,8 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
 
   const T A = tb->A[rqual[n - 1]];
   const T k2 = sc.k2, x = sc.x, c0 = sc.c, gfin = sc.gfin;
-  int E = 0;          // total power-of-two renormalisation of the strips
-  bool fail = false;  // a strip boundary underflowed
+  int E = 0;          // total power-of-two scaling: strip renormalisations (and the drift tier's row boosts)
+  bool fail = false;  // a strip boundary left the range
 
   // drift tier: per-row power-of-two boosts, strips re-run when they leave the
   // window; the scratch holds two boundaries (read one, write the other)
@@ -160,9 +160,10 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   int strip_lg = 0;     // drift: exponent of the strip's bottom maximum (or +-1024: inf / zero)
   double zkeep = 0.0;   // drift: the last strip's final sum, on lane 31
 
-  // One strip of rows.  FIRST and LAST are compile-time tags, so the steady
-  // loop carries no per-step test of the strip position.  Returns false when
-  // the strip's bottom boundary underflowed.
+  // One strip of rows (Bs: the drift tier's boost bits for the strip, else 0).
+  // FIRST and LAST are compile-time tags, so the steady loop carries no
+  // per-step test of the strip position.  Returns false when the strip's
+  // bottom boundary left [strip_floor, strip_ceil).
   auto run_strip = [&](auto first_tag, auto last_tag, const int strip, const int Bs) -> bool {
     constexpr bool FIRST = decltype(first_tag)::value;
     constexpr bool last = decltype(last_tag)::value;
