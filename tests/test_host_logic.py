@@ -158,3 +158,62 @@ def test_prefix_plan_guards(built_library):
         native.prefix_plan(np.zeros(4, np.uint8), np.array([0, 3, 2], np.int64))
     order, share = native.prefix_plan(np.zeros(1, np.uint8), np.array([0], np.int64))
     assert len(order) == 0 and len(share) == 0
+
+
+def _folded_forward(read, qual, hap, gap, ext, boost=None):
+    """The kernels' folded, row-scaled semiglobal recurrence in float64 (per row i: mu = s_above x
+    (hit | miss), om = mu_left + x om, u = mu + X nu, s = mu + K nu + k2 om; row 0 = c; the last
+    row's X is alpha f_n, so its u is the scaled M + I), with optional per-row boosts 2^k_i on
+    hit, miss, K and X as the drift tier applies them.  Returns ln L."""
+    a, alpha = 1.0 - 2.0 * gap, 0.25 * gap
+    k1, k2, x4 = (1.0 - ext) * alpha / a, (1.0 - ext) * gap / a, 0.25 * ext
+    e = 10.0 ** (-np.minimum(np.asarray(qual, np.float64), 60.0) / 10.0)
+    p1, p0 = 1.0 - e, e / 3.0
+    mx = np.maximum(p1, p0)
+    f = 1.0 / (a * mx)
+    hit, miss, K, X = p1 / mx, p0 / mx, k1 * f, x4 * f
+    X = X.copy()
+    X[-1] = alpha * f[-1]
+    k = np.zeros(len(read), np.int64) if boost is None else np.asarray(boost, np.int64)
+    scale = np.ldexp(1.0, k)
+    hit, miss, K, X = hit * scale, miss * scale, K * scale, X * scale
+    c = 2.0 ** 20
+    m = len(hap)
+    s_prev = np.full(m + 1, c)   # row 0: s and u are c in every column
+    u_prev = np.full(m + 1, c)
+    hb = np.frombuffer(hap.encode(), np.uint8)
+    rb = np.frombuffer(read.encode(), np.uint8)
+    for i in range(len(read)):
+        match = np.concatenate([[False], hb == rb[i]])   # column 0 has no base
+        diag = np.concatenate([[0.0], s_prev[:-1]])
+        mu = diag * np.where(match, hit[i], miss[i])
+        nu = u_prev
+        om = np.zeros(m + 1)
+        for j in range(1, m + 1):
+            om[j] = mu[j - 1] + ext * om[j - 1]
+        u = mu + X[i] * nu
+        s = mu + K[i] * nu + k2 * om
+        s_prev, u_prev = s, u
+    Z = u_prev.sum()
+    return np.log(Z) - np.log(c) - np.log(m + 1) + np.sum(np.log(a * mx)) - k.sum() * np.log(2.0)
+
+
+def test_drift_boosts_cancel_exactly():
+    """The drift tier's per-row powers of two leave ln L unchanged: the folded recurrence with
+    random boosts 2^k_i (k_i in 0..3) equals the unboosted one, and both equal the FP64 oracle."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(11)
+    for _ in range(4):
+        hap = "".join(rng.choice(list("ACGT"), int(rng.integers(30, 80))))
+        n = int(rng.integers(10, 40))
+        start = int(rng.integers(0, len(hap) - n + 1))
+        read = list(hap[start:start + n])
+        for i in np.flatnonzero(rng.random(n) < 0.1):
+            read[i] = "ACGT"[("ACGT".index(read[i]) + 1) % 4]
+        read = "".join(read)
+        qual = rng.choice([10, 20, 30, 40], n).astype(np.uint8)
+        plain = _folded_forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10)
+        boosted = _folded_forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10, boost=rng.integers(0, 4, n))
+        want = O.forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10)
+        assert abs(boosted - plain) <= 1e-12 * abs(plain)
+        assert abs(plain - want) <= 1e-9 * abs(want)
