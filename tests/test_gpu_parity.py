@@ -97,7 +97,7 @@ def test_edge_cases(mixed, fp64, anchored):
 
 
 @pytest.mark.parametrize("name", ["single_region_q45", "single_region_q30"])
-def test_config0_against_reference(mixed, name):
+def test_single_region_against_reference(mixed, name):
     d = golden(name)
     packed = native.Packed(d["read_bases"], d["read_quals"], d["read_off"], d["hap_bases"], d["hap_off"],
                            region_read_off=d["region_read_off"], region_hap_off=d["region_hap_off"])
@@ -134,7 +134,7 @@ def _argmax_agree(w, got, want):
     return agree, total
 
 
-def test_config1_sample_against_oracle(mixed):
+def test_batched_regions_sample_against_oracle(mixed):
     w = S.batched_regions(n_regions=24)
     got = _with(mixed, w.gap, w.ext).score_packed(_packed(w))
     want = _oracle_workload(w)
@@ -179,7 +179,7 @@ def test_anchored_refinement_windows(mixed, fp64):
           f"rescued {mixed.last['float64_fallback_pairs']}")
 
 
-def test_config2_precision_stress(mixed):
+def test_long_haplotype_stress_precision(mixed):
     w = S.long_haplotype_stress(n_regions=6)
     got = _with(mixed, w.gap, w.ext).score_packed(_packed(w))
     want = _oracle_workload(w)

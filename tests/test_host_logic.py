@@ -62,7 +62,7 @@ def test_quality_objects_are_validated_once_and_kept():
     assert out[0][1] is out[1][1] and out[0][1].dtype == np.uint8
 
 
-def test_config0_shape():
+def test_single_region_shape():
     w = S.single_region()
     assert w.n_regions == 1 and len(w.read_off) - 1 == 64 and list(w.hap_lengths()) == [300, 297]
     assert set(np.unique(w.read_quals)) <= {10, 20, 30, 40}
@@ -70,7 +70,7 @@ def test_config0_shape():
     assert abs(w.gap - 10 ** -4.5) < 1e-18 and w.ext == 0.1
 
 
-def test_config1_shape_small():
+def test_batched_regions_shape_small():
     w = S.batched_regions(n_regions=40)
     nh = np.diff(w.region_hap_off)
     nr = np.diff(w.region_read_off)
