@@ -4,7 +4,7 @@
  *
  * Results are natural-log likelihoods (float64), like every reference entry
  * point; an empty read or haplotype gives -inf.  Status codes follow the
- * reference's C ABI (caller/native/caller/batch_hmm.cpp:217-219,
+ * reference's C ABI (caller/native/caller/batch_hmm.cpp:192-199,
  * trie_vector.cpp:284-286): 0 = OK, 1 = bad arguments; codes >= 2 are device
  * errors this library adds.  vd_last_error() describes the last failure of
  * the calling thread.  All inputs are caller-owned host memory (device memory
@@ -70,7 +70,7 @@ typedef struct vd_params {
  *    order, each a reads x haplotypes row-major block (trie_vector.cpp:284-292
  *    layout, one block per region); or
  *  - as explicit pairs (pair_read != NULL): out[p] scores read pair_read[p]
- *    against haplotype pair_hap[p] (batch_hmm.cpp:217 semantics). */
+ *    against haplotype pair_hap[p] (batch_hmm.cpp:192 semantics). */
 typedef struct vd_batch {
   const unsigned char *read_bases;
   const unsigned char *read_quals;
@@ -178,7 +178,7 @@ int vd_plan_destroy(vd_plan *plan);
  * gap 0.001 / ext 0.1 of the batch kernels is kept where the reference
  * hard-codes it. */
 
-/* caller/native/caller/batch_hmm.cpp:217 pairhmm_pairs: count independent pairs,
+/* caller/native/caller/batch_hmm.cpp:192 pairhmm_pairs: count independent pairs,
  * mode 0/2 semiglobal, 1 anchored; lanes is accepted and ignored. */
 int vd_pairhmm_pairs(const char *const *reads, const unsigned char *const *quals, const int *rn,
                      const char *const *haps, const int *hn, int count, int mode, int lanes,

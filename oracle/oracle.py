@@ -312,7 +312,7 @@ def ref_core_pair_scores(s: str, q, haps) -> np.ndarray:
 
 
 def ref_pairhmm_pairs(jobs, mode=0, lanes=0) -> np.ndarray:
-    """batch_hmm.cpp:217 with the argument layout of cpu_batch._uncached_pairs (cpu_batch.py:44-62)."""
+    """batch_hmm.cpp:192 with the argument layout of cpu_batch._uncached_pairs (cpu_batch.py:44-62)."""
     count = len(jobs)
     enc = [(s.encode(), _q(q).tobytes(), h.encode()) for s, q, h in jobs]
     reads = (ctypes.c_char_p * count)(*(e[0] for e in enc))

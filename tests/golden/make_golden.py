@@ -13,7 +13,7 @@ used).  Shapes and seeds are those of the reference's tests:
   catalog_seed7713.npz tests/test_cpu_catalog.py:22-31  (anchored_pairhmm values)
   edge_cases.npz       tests/test_accelerator.py:21-40 shapes plus N bases, Q0/Q1/Q255,
                        1x1 and empty pairs
-  single_region_q45.npz      the single-region workload workload (seed 0) at gap 10^-4.5 / ext 0.1 through
+  single_region_q45.npz      the single-region workload (seed 0) at gap 10^-4.5 / ext 0.1 through
                        wide.cpp read_haplotype_batch_mode
   single_region_q30.npz      the same reads at the production 0.001 / 0.1 through
                        cpu_batch.pairs (trie_many, the production CPU path)
@@ -22,13 +22,14 @@ used).  Shapes and seeds are those of the reference's tests:
                        with seeded mapping qualities, triangular._diploid_likelihood_numpy (no
                        prior) and mixture_cpu.general (mixture_general.cpp) at priors 0 and 0.001
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [REFERENCE_CHECKOUT]
 """
 from __future__ import annotations
 
 import ctypes
 import importlib.machinery
 import importlib.util
+import os
 import sys
 import types
 from pathlib import Path
@@ -38,7 +39,10 @@ import numpy as np
 sys.dont_write_bytecode = True
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REFERENCE = Path("/root/reference/caller/native/caller")
+# the reference checkout: first command-line argument, else $VARDEPTH_REFERENCE, else the build
+# container's read-only copy
+REFERENCE = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("VARDEPTH_REFERENCE", "/root/reference")) \
+    / "caller" / "native" / "caller"
 sys.path.insert(0, str(ROOT))
 
 from oracle import oracle as O  # noqa: E402

@@ -56,7 +56,7 @@ def test_engine_argument_errors(built_library):
     h = ctypes.c_void_p()
     assert lib.vd_engine_create(0, 4, ctypes.byref(h)) == native.VD_EINVAL  # budget below 8 MiB
     assert b"8 MiB" in lib.vd_last_error()
-    # reference return code 1 for bad arguments (batch_hmm.cpp:219)
+    # reference return code 1 for bad arguments (batch_hmm.cpp:194)
     assert lib.vd_pairhmm_pairs(None, None, None, None, None, -1, 0, 0, None) == 1
     assert lib.vd_pairhmm_pairs(None, None, None, None, None, 1, 3, 0, None) == 1
     assert lib.vd_trie_many(None, None, None, -1, None, None, 0, 0, 0, None, None) == 1
