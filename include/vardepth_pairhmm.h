@@ -293,8 +293,11 @@ int vd_region_genotypes(vd_engine *engine, const vd_batch *batch, const vd_param
  * the array's device address and the grid sizes, so make that first call
  * before any stream capture.  Every call shares the one array (the previous
  * call's contents stay in it; each call clears what must start at zero), so
- * overlapping calls would race on it and must not happen; calls from several
- * host threads of one process are serialised by a lock. */
+ * overlapping calls on one device would race on it and must not happen; calls
+ * from several host threads on the same device are serialised by a per-device
+ * lock.  Every buffer must be device (or managed) memory of `device`, checked
+ * with cudaPointerGetAttributes before anything is enqueued (VD_EINVAL
+ * otherwise). */
 int vd_forward_region_noalloc(int device, const unsigned char *read_bases,
                               const unsigned char *read_quals, const int64_t *read_off,
                               int64_t n_reads, const unsigned char *hap_bases,

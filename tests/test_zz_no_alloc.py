@@ -2,10 +2,12 @@
 
 It scores one region (every read against every haplotype) from device buffers
 the caller owns, with all scratch in the library's fixed static device array.
-Its results must agree with vd_forward on the same region, within the tests'
-tolerances: |delta log10 L| <= 1e-4 per pair for precision 'mixed' and 2e-9
-in ln for 'float64', with identical -inf entries, on two calls in a row (the
-second call finds the first call's contents still in the shared array).
+Its results must agree with vd_forward on the same region and with the FP64
+oracle, within the tests' tolerances: |delta log10 L| <= 1e-4 per pair for
+precision 'mixed' and 2e-9 in ln for 'float64', with identical -inf entries,
+on two calls in a row (the second call finds the first call's contents still
+in the shared array).  A call after the first leaves the device's free memory
+unchanged, and host pointers are refused before anything runs.
 
 The file name sorts last so that it also runs after every other test in the
 same process; it must pass alone in a fresh process as well.
@@ -16,6 +18,7 @@ import numpy as np
 import pytest
 
 from conftest import FP64_ATOL_LN, LN10
+from oracle import oracle as O
 from vardepth_b200 import native
 
 pytestmark = pytest.mark.gpu
@@ -79,6 +82,15 @@ def expected(region, anchored: bool, precision: int) -> np.ndarray:
     return out
 
 
+def oracle_region(region, anchored: bool) -> np.ndarray:
+    """The FP64 oracle on every (read, haplotype) pair, reads x haplotypes row-major."""
+    rb, rq, ro, hb, ho = region
+    nr, nh = len(ro) - 1, len(ho) - 1
+    pr = np.repeat(np.arange(nr, dtype=np.int32), nh)
+    ph = np.tile(np.arange(nh, dtype=np.int32), nr)
+    return O.forward_pairs(rb, rq, ro, hb, ho, pr, ph, 0.001, 0.1, anchored=anchored, threads=0)
+
+
 def call_noalloc(region, anchored: bool, precision: int, stream=None):
     """Upload the region into caller-owned device buffers and score it."""
     import torch
@@ -107,13 +119,61 @@ def assert_agree(got, want, precision):
 
 @pytest.mark.parametrize("precision", [native.VD_PRECISION_MIXED, native.VD_PRECISION_FLOAT64])
 @pytest.mark.parametrize("anchored", [False, True])
-def test_noalloc_matches_vd_forward_twice(anchored, precision):
+def test_noalloc_matches_vd_forward_and_the_oracle_twice(anchored, precision):
     region = make_region(11 + int(anchored), 96, 12, anchored)
     want = expected(region, anchored, precision)
+    oracle = oracle_region(region, anchored)
     for _ in range(2):  # the second call finds the first call's scratch contents
         rc, got = call_noalloc(region, anchored, precision)
         assert rc == native.VD_OK, native.last_error()
         assert_agree(got, want, precision)
+        assert_agree(got, oracle, precision)
+
+
+def test_noalloc_leaves_free_device_memory_unchanged():
+    """After a first call (which loads the kernels), a call changes neither the device's free
+    memory (cudaMemGetInfo) nor torch's allocator: all of its scratch is the static array."""
+    import torch
+    region = make_region(21, 120, 10, False)
+    rb, rq, ro, hb, ho = region
+    nr, nh = len(ro) - 1, len(ho) - 1
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (rb, rq, ro, hb, ho)]
+    out = torch.empty(nr * nh, dtype=torch.float64, device="cuda")
+    params, _keep = native.make_params(0.001, 0.1, False, native.VD_PRECISION_MIXED)
+    lib = native.library()
+    args = (0, dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), nr, dev[3].data_ptr(), dev[4].data_ptr(),
+            nh, ctypes.byref(params), out.data_ptr(), None)
+    assert lib.vd_forward_region_noalloc(*args) == native.VD_OK, native.last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    assert lib.vd_forward_region_noalloc(*args) == native.VD_OK, native.last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+    assert torch.cuda.memory_reserved() == reserved0
+    assert_agree(out.cpu().numpy(), oracle_region(region, False), native.VD_PRECISION_MIXED)
+
+
+def test_noalloc_refuses_host_pointers():
+    """Host buffers are refused with VD_EINVAL before anything is enqueued."""
+    import torch
+    rb, rq, ro, hb, ho = make_region(22, 16, 3, False)
+    nr, nh = len(ro) - 1, len(ho) - 1
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (rb, rq, ro, hb, ho)]
+    out_dev = torch.empty(nr * nh, dtype=torch.float64, device="cuda")
+    out_host = np.empty(nr * nh, np.float64)
+    params, _keep = native.make_params(0.001, 0.1, False, native.VD_PRECISION_MIXED)
+    lib = native.library()
+    host_reads = np.ascontiguousarray(rb)
+    rc = lib.vd_forward_region_noalloc(0, host_reads.ctypes.data, dev[1].data_ptr(), dev[2].data_ptr(), nr,
+                                       dev[3].data_ptr(), dev[4].data_ptr(), nh, ctypes.byref(params),
+                                       out_dev.data_ptr(), None)
+    assert rc == native.VD_EINVAL and "read_bases" in native.last_error()
+    rc = lib.vd_forward_region_noalloc(0, dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), nr,
+                                       dev[3].data_ptr(), dev[4].data_ptr(), nh, ctypes.byref(params),
+                                       out_host.ctypes.data, None)
+    assert rc == native.VD_EINVAL and "out" in native.last_error()
 
 
 def test_noalloc_on_a_caller_stream_after_a_different_region():

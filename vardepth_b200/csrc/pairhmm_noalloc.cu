@@ -18,8 +18,13 @@
 // kernels from then on.  That first call should come before any stream capture.
 // Every call reuses the same array and finds the previous call's contents in
 // it: the counters that must start at zero are cleared at the start of each
-// call, the lists are read only up to those counters.  Overlapping calls would
-// race on the array; calls from several host threads are serialised by a lock.
+// call, the lists are read only up to those counters.  Overlapping calls on
+// one device would race on its array; calls from several host threads on the
+// same device are serialised by a per-device lock (calls on different devices
+// use different arrays and run side by side).  The caller's buffers are
+// checked to be device memory of the chosen device before anything is
+// enqueued, and a call that fails after enqueueing work waits for it before
+// returning.
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -74,7 +79,7 @@ __global__ void na_prep_haps(const int64_t* __restrict__ hap_off, int n_haps, un
     int keep = 0;
     if (h < n_haps) {
       const int64_t m = hap_off[h + 1] - hap_off[h];
-      if (m > kNaMaxHapLen || m < 0) atomicExch(&cnt[8], 2ull);
+      if (m > kNaMaxHapLen || m < 0) atomicCAS(&cnt[8], 0ull, 2ull);  // the first limit found is reported
       keep = m > 0 ? 1 : 0;
     }
     // block-wide exclusive scan of keep (order-preserving compaction)
@@ -123,7 +128,7 @@ __global__ void na_prep_reads(const unsigned char* __restrict__ read_quals, cons
   for (int64_t r = tid; r < n_reads; r += stride) {
     const int64_t o = read_off[r];
     const int64_t n = read_off[r + 1] - o;
-    if (n > kNaMaxReadLen || n < 0) atomicExch(&cnt[8], 1ull);
+    if (n > kNaMaxReadLen || n < 0) atomicCAS(&cnt[8], 0ull, 1ull);
     bool gen = false;
     for (int64_t i = 0; i < n && i < kNaMaxReadLen; ++i) gen |= tab->general[read_quals[o + i]] != 0;
     const int rows = (int)n + anchored;
@@ -185,6 +190,9 @@ namespace vd {
 namespace {
 
 struct NaDevice {
+  std::mutex mu;                     // one call at a time on this device: the calls share its scratch
+  Tables<float> t32;                 // staging of the model tables (filled on the host, copied into the scratch)
+  Tables<double> t64;
   bool ready = false;
   unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch on this device
   int grid32[2] = {0, 0};            // [anchored] blocks of na_primary<float>
@@ -193,11 +201,6 @@ struct NaDevice {
 };
 constexpr int kNaMaxDevices = 64;
 NaDevice g_na[kNaMaxDevices];
-std::mutex g_na_mu;  // one call at a time: the calls share the scratch and the host tables
-
-// staging of the model tables (filled on the host, copied into the scratch)
-Tables<float> g_na_t32;
-Tables<double> g_na_t64;
 
 int na_fail(int code, const std::string& msg) { return report_error(code, msg.c_str()); }
 
@@ -211,6 +214,18 @@ int na_cuda(cudaError_t e, const char* what) {
     cudaError_t na_err_ = (call);                           \
     if (na_err_ != cudaSuccess) return na_cuda(na_err_, #call); \
   } while (0)
+
+// A caller buffer must be device (or managed) memory of the call's device: a
+// host pointer handed to the kernels would fault.  cudaPointerGetAttributes
+// allocates nothing.
+bool na_on_device(const void* p, int device) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
+}
 
 // Per-device set-up, with the device current: the scratch address and the
 // grid sizes.  Runs during the first call on the device.
@@ -269,7 +284,7 @@ extern "C" int vd_forward_region_noalloc(int device, const unsigned char* read_b
     return na_fail(VD_EINVAL, "NULL device pointer");
   if (device < 0 || device >= kNaMaxDevices) return na_fail(VD_ENODEV, "device index out of range");
 
-  std::lock_guard<std::mutex> lk(g_na_mu);
+  std::lock_guard<std::mutex> lk(g_na[device].mu);
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
   if (cudaSetDevice(device) != cudaSuccess) {
@@ -283,7 +298,22 @@ extern "C" int vd_forward_region_noalloc(int device, const unsigned char* read_b
   int rc = na_setup(device);
   if (rc) return rc;
   NaDevice& d = g_na[device];
+  {
+    const void* bufs[6] = {read_bases, read_quals, read_off, hap_bases, hap_off, out};
+    static const char* names[6] = {"read_bases", "read_quals", "read_off", "hap_bases", "hap_off", "out"};
+    for (int i = 0; i < 6; ++i)
+      if (!na_on_device(bufs[i], device))
+        return na_fail(VD_EINVAL, std::string("vd_forward_region_noalloc: ") + names[i] +
+                                      " is not device memory of the selected device");
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // once work is enqueued, an early return waits for it first: kernels still
+  // running would otherwise share the scratch with the next call
+  struct Drain {
+    cudaStream_t s;
+    bool armed = false;
+    ~Drain() { if (armed) { cudaStreamSynchronize(s); cudaGetLastError(); } }
+  } drain{s};
   unsigned char* sc = d.scratch;
   const bool anch = params->anchored != 0;
   const bool f64 = params->precision == VD_PRECISION_FLOAT64;
@@ -292,9 +322,10 @@ extern "C" int vd_forward_region_noalloc(int device, const unsigned char* read_b
   // so the staging tables are not rewritten while the copy is pending
   Scalars<float> s32;
   Scalars<double> s64;
-  build_model_tables(params->gap, params->ext, params->quality_offsets, &g_na_t32, &g_na_t64, &s32, &s64);
-  NA_CUDA(cudaMemcpyAsync(sc + kOffTab32, &g_na_t32, sizeof(g_na_t32), cudaMemcpyHostToDevice, s));
-  NA_CUDA(cudaMemcpyAsync(sc + kOffTab64, &g_na_t64, sizeof(g_na_t64), cudaMemcpyHostToDevice, s));
+  build_model_tables(params->gap, params->ext, params->quality_offsets, &d.t32, &d.t64, &s32, &s64);
+  drain.armed = true;
+  NA_CUDA(cudaMemcpyAsync(sc + kOffTab32, &d.t32, sizeof(d.t32), cudaMemcpyHostToDevice, s));
+  NA_CUDA(cudaMemcpyAsync(sc + kOffTab64, &d.t64, sizeof(d.t64), cudaMemcpyHostToDevice, s));
   // the previous call's counters and lists are still in the array: the
   // counters are cleared here; the lists are only read up to their counts
   NA_CUDA(cudaMemsetAsync(sc + kOffCnt, 0, 16 * sizeof(unsigned long long), s));
@@ -361,6 +392,7 @@ extern "C" int vd_forward_region_noalloc(int device, const unsigned char* read_b
   unsigned long long h[16];
   NA_CUDA(cudaMemcpyAsync(h, sc + kOffCnt, sizeof(h), cudaMemcpyDeviceToHost, s));
   NA_CUDA(cudaStreamSynchronize(s));
+  drain.armed = false;
   if (h[8] == 1) return na_fail(VD_EINVAL, "vd_forward_region_noalloc: reads are limited to 255 bases");
   if (h[8] == 2) return na_fail(VD_EINVAL, "vd_forward_region_noalloc: haplotypes are limited to 1023 bases");
   if (h[5]) return na_fail(VD_EOVERFLOW, "rescue list overflow");
