@@ -22,9 +22,19 @@ read against every haplotype of its region.
            caller/native/caller/wide.cpp) read_haplotype_batch_mode on every host
            core, on a deterministic region subsample of the same workload.
 
+  parity   GPU results against the reference's own outputs on the whole CPU sample
+           (vs_reference) and against the FP64 oracle on at least 1e10 cells of it
+           (vs_oracle), with the genotype argmax of every checked region; for the
+           mixed-length workload also a long_read block of 20 regions of 1-10 kb reads.
+  e2e_pairs  GCUPS of score_pairs(list of (read, qualities, haplotype)) -- the
+           reference's Python drop-in signature -- on a region sample of >= 1e6 pairs.
+
 --impl reference times only that CPU implementation (rank 0), one subsample pass
-per step.  Multi-GPU: one process per GPU under torchrun, each rank scores its
-own copy of the workload (weak scaling, no data-path collective).
+per step.  Multi-GPU: one process per GPU under torchrun; every rank builds the
+same workload, regions go to ranks longest-processing-time first by DP cells
+(vardepth_b200/shard.py) and each rank scores its shard (strong scaling, no
+data-path collective); the e2e results land in a node-wide shared-memory array,
+each rank writing its own slices.
 """
 from __future__ import annotations
 
@@ -166,7 +176,7 @@ def cpu_reference(w, seconds, repeats=1, per_step=False):
         model = platform.processor()
     sample = (f"{k2} of {w.n_regions} regions (seeded order), {cells:.3e} cells, "
               f"read_haplotype_batch_mode (AVX-512 8-lane) on {threads} threads, {model}")
-    return dict(cells=cells, times=times, threads=threads, sample=sample, jobs=jobs)
+    return dict(cells=cells, times=times, threads=threads, sample=sample, jobs=jobs, regions=order[:k2])
 
 
 def _diploid_gl(ll):
@@ -329,6 +339,58 @@ def gradient_arm(args, local):
     engine.close()
 
 
+def _region_offsets(w):
+    return np.concatenate([[0], np.cumsum(np.diff(w.region_read_off) * np.diff(w.region_hap_off))])
+
+
+def _compare(w, got, regions, want, region_cells):
+    """|dlog10 L| of the GPU outputs of `regions` (in that order) against `want`, and the
+    genotype argmax of each region (sum over reads of ln((L_a + L_b) / 2))."""
+    offs = _region_offsets(w)
+    idx = np.concatenate([np.arange(offs[g], offs[g + 1]) for g in regions])
+    a, b = got[idx], want
+    fin = np.isfinite(b)
+    if not np.array_equal(np.isneginf(a), np.isneginf(b)) or not np.all(np.isfinite(a[fin])):
+        raise SystemExit("-inf / non-finite results differ from the checker's")
+    err = np.abs(a[fin] - b[fin]) / np.log(10.0)
+    agree, o = 0, 0
+    for g in regions:
+        nr = int(w.region_read_off[g + 1] - w.region_read_off[g])
+        nh = int(w.region_hap_off[g + 1] - w.region_hap_off[g])
+        if nr and nh:
+            x, y = a[o:o + nr * nh].reshape(nr, nh), b[o:o + nr * nh].reshape(nr, nh)
+            agree += int(np.argmax(_diploid_gl(x)) == np.argmax(_diploid_gl(y)))
+        else:
+            agree += 1
+        o += nr * nh
+    return {"regions": int(len(regions)), "pairs": int(len(idx)), "cells": int(region_cells[regions].sum()),
+            "max_abs_dlog10": float(err.max()) if err.size else 0.0,
+            "p99_abs_dlog10": float(np.quantile(err, 0.99)) if err.size else 0.0,
+            "genotype_argmax_agree": int(agree)}
+
+
+def _oracle(w, regions):
+    from oracle import oracle as O
+    sw = w.subset(regions)
+    pr, ph = sw.explicit_pairs()
+    return O.forward_pairs(sw.read_bases, sw.read_quals, sw.read_off, sw.hap_bases, sw.hap_off, pr, ph, w.gap,
+                           w.ext, threads=0)
+
+
+def _pair_list(w, regions):
+    """The regions as the reference's callers hand them over: a list of (read str, quality
+    bytes, haplotype str), every read against every haplotype of its region."""
+    out = []
+    for g in regions:
+        haps = [bytes(w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]]).decode()
+                for h in range(w.region_hap_off[g], w.region_hap_off[g + 1])]
+        for r in range(w.region_read_off[g], w.region_read_off[g + 1]):
+            a, b = w.read_off[r], w.read_off[r + 1]
+            seq, q = bytes(w.read_bases[a:b]).decode(), bytes(w.read_quals[a:b])
+            out.extend((seq, q, h) for h in haps)
+    return out
+
+
 def main():
     args = parse()
     if args.regions <= 0:
@@ -341,30 +403,38 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    torch.cuda.set_device(local)
 
-    from vardepth_b200 import native
+    from vardepth_b200 import native, shard
     if args.workload == "planted_error_model":
         gradient_arm(args, local)
         return
     w = make_workload(args.workload, args.regions)
     cells, pairs = w.cells(), w.pairs()
+    full = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
+                         region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
+    # this rank's regions: all of them on one GPU, its LPT shard on several
+    if world > 1:
+        shards = shard.shard_regions(shard.region_cells(full), world)
+        mine, positions = shard.subset(full, shards[rank])
+    else:
+        shards, mine, positions = None, full, None
+    my_cells = int(shard.region_cells(mine).sum()) if mine.n_outputs() else 0
 
     def pinned(a):
-        t = torch.empty(a.nbytes, dtype=torch.uint8).pin_memory()
-        v = t.numpy().view(a.dtype)
+        t = torch.empty(max(1, a.nbytes), dtype=torch.uint8).pin_memory()
+        v = t.numpy()[:a.nbytes].view(a.dtype)
         v[:] = a.reshape(-1)
         return t, v
 
     keep = []
     arrays = {}
     for name in ("read_bases", "read_quals", "read_off", "hap_bases", "hap_off", "region_read_off", "region_hap_off"):
-        t, v = pinned(getattr(w, name))
+        t, v = pinned(getattr(mine, name))
         keep.append(t)
         arrays[name] = v
     packed = native.Packed(arrays["read_bases"], arrays["read_quals"], arrays["read_off"], arrays["hap_bases"],
@@ -375,6 +445,7 @@ def main():
     params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
     peak = __import__("ctypes").c_double()
     native.check(native.library().vd_measure_fp32_peak(local, __import__("ctypes").byref(peak)), "fp32 peak")
+    warm = max(3, args.warmup)
 
     def barrier():
         if dist is not None:
@@ -386,6 +457,14 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    def gather_all(x):
+        if dist is None:
+            return [x]
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        parts = torch.empty(world, dtype=torch.float64, device="cuda")
+        dist.all_gather_into_tensor(parts, t)
+        return parts.tolist()
 
     # ---- autotuner: work-list choices timed on a region sample, kept on the engine ----
     tuned = None
@@ -401,19 +480,10 @@ def main():
                  "sample_regions": sub.n_regions, "sample_cells": sub.cells(),
                  "sample_ms_default": best.get("default_ms"), "sample_ms_chosen": best.get("sample_ms"),
                  "trials": tlog, "seconds": round(time.perf_counter() - t0, 2)}
-        if tuned["chosen"] != autotune.DEFAULT:
-            # the untuned schedule on the full batch, for the record
-            saved = engine.tuning()
-            engine.set_tuning(**autotune.DEFAULT)
-            uplan = engine.plan(packed, params)
-            uplan.run()
-            tuned["untuned_full_gcups"] = round(cells / uplan.run().kernel_ms / 1e6, 3)
-            uplan.close()
-            engine.set_tuning(**saved)
 
     # ---- device-resident batches (value) ----
     plan = engine.plan(packed, params)
-    for _ in range(max(3, args.warmup)):
+    for _ in range(warm):
         plan.run()
     uuid = None
     try:
@@ -426,10 +496,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     kernel_ms = primary_ms = 0.0
-    rescued = 0
-    drift_rescued = 0
-    launches = 0
-    shared = 0
+    rescued = drift_rescued = launches = shared = 0
     for _ in range(args.steps):
         st = plan.run()
         kernel_ms += st.kernel_ms
@@ -441,11 +508,18 @@ def main():
     torch.cuda.synchronize()
     barrier()
     sampler.stop()
-    kernel_ms = allmax(kernel_ms)
-    step_ms = kernel_ms / args.steps
-    value = world * cells / (step_ms / 1e3) / 1e9
+    rank_ms = gather_all(kernel_ms / args.steps)
+    step_ms = max(rank_ms)
+    value = cells / (step_ms / 1e3) / 1e9
     got = plan.fetch()
     plan.close()
+    sharding = None
+    if world > 1:
+        rank_cells = gather_all(float(my_cells))
+        sharding = {"policy": "LPT by DP cells (vardepth_b200/shard.py)", "ranks": world,
+                    "rank_cells": [int(c) for c in rank_cells], "rank_kernel_ms": [round(x, 3) for x in rank_ms],
+                    "imbalance_ms_max_over_mean": round(max(rank_ms) / (sum(rank_ms) / world), 4),
+                    "imbalance_cells_max_over_mean": round(max(rank_cells) / (sum(rank_cells) / world), 4)}
 
     # ---- plain schedule on the same resident inputs (the batched-vs-plain comparison) ----
     plain = None
@@ -453,7 +527,7 @@ def main():
         plain_params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED,
                                              schedule=native.VD_SCHEDULE_PLAIN)
         pplan = engine.plan(packed, plain_params)
-        for _ in range(args.warmup):
+        for _ in range(warm):
             pplan.run()
         barrier()
         torch.cuda.synchronize()
@@ -471,7 +545,7 @@ def main():
         pplan.close()
         if not np.array_equal(plain_got, got, equal_nan=True):
             raise SystemExit("plain and batched schedules disagree")
-        plain_value = world * cells / (plain_ms / 1e3) / 1e9
+        plain_value = cells / (plain_ms / 1e3) / 1e9
         plain = {"value": round(plain_value, 3), "unit": "GCUPS", "ms_per_step": round(plain_ms, 3),
                  "steps": plain_steps, "gpu_launches": plain_launches,
                  "batched_over_plain": round(value / plain_value, 3),
@@ -479,37 +553,20 @@ def main():
                              "input order, static round-robin over a fixed grid; same tiers and "
                              "arithmetic, results bit-identical to the batched schedule"}
 
-    # ---- parity spot check on a region subsample (oracle, CPU) ----
-    parity = None
-    if rank == 0:
-        from oracle import oracle as O
-        sub = np.random.default_rng(7).choice(w.n_regions, size=min(24, w.n_regions), replace=False)
-        offs = np.concatenate([[0], np.cumsum(np.diff(w.region_read_off) * np.diff(w.region_hap_off))])
-        idx = np.concatenate([np.arange(offs[g], offs[g + 1]) for g in sub])
-        sw = w.subset(sub)
-        pr, ph = sw.explicit_pairs()
-        want = O.forward_pairs(sw.read_bases, sw.read_quals, sw.read_off, sw.hap_bases, sw.hap_off, pr, ph, w.gap,
-                               w.ext, threads=0)
-        err = np.abs(got[idx] - want) / np.log(10.0)
-        # genotype-likelihood argmax per region (sum over reads of ln((L_a + L_b) / 2))
-        agree, o = 0, 0
-        for g in sub:
-            nr = int(w.region_read_off[g + 1] - w.region_read_off[g])
-            nh = int(w.region_hap_off[g + 1] - w.region_hap_off[g])
-            a = got[offs[g]:offs[g + 1]].reshape(nr, nh)
-            b = want[o:o + nr * nh].reshape(nr, nh)
-            agree += int(np.argmax(_diploid_gl(a)) == np.argmax(_diploid_gl(b)))
-            o += nr * nh
-        parity = {"pairs_checked": int(len(idx)), "max_abs_dlog10": float(err.max()),
-                  "p99_abs_dlog10": float(np.quantile(err, 0.99)), "oracle": "FP64 restatement (oracle/)",
-                  "regions_checked": int(len(sub)), "genotype_argmax_agree": int(agree)}
-
     # ---- end to end through vd_forward with pinned host buffers (e2e) ----
     e2e = None
     if not args.no_e2e:
-        out_t = torch.empty(pairs * 8, dtype=torch.uint8).pin_memory()
-        out = out_t.numpy().view(np.float64)
-        for _ in range(max(1, args.warmup)):
+        out_t = torch.empty(max(1, mine.n_outputs()) * 8, dtype=torch.uint8).pin_memory()
+        out = out_t.numpy().view(np.float64)[:mine.n_outputs()]
+        shared_out = None
+        if world > 1:
+            name = f"vd_bench_{os.environ.get('MASTER_PORT', '0')}_{os.getppid()}"
+            if rank == 0:
+                shared_out = shard.SharedOutput(name, pairs, create=True)
+            barrier()
+            if rank != 0:
+                shared_out = shard.SharedOutput(name, pairs, create=False)
+        for _ in range(warm):
             engine.forward(packed, params, out)
         barrier()
         torch.cuda.synchronize()
@@ -518,23 +575,102 @@ def main():
         for _ in range(args.steps):
             t0 = time.perf_counter()
             _, st = engine.forward(packed, params, out)
+            if shared_out is not None:
+                shared_out.write(positions, out)   # this rank's slices of the full output vector
             wall += time.perf_counter() - t0
         torch.cuda.synchronize()
         barrier()
         wall = allmax(wall)
-        e2e = {"value": round(world * cells / (wall / args.steps) / 1e9, 3), "unit": "GCUPS",
+        e2e = {"value": round(cells / (wall / args.steps) / 1e9, 3), "unit": "GCUPS",
                "h2d_bytes_per_step": int(st.h2d_bytes), "d2h_bytes_per_step": int(st.d2h_bytes),
                "ms_per_step": round(1e3 * wall / args.steps, 3), "host_ms_per_step": round(st.host_ms, 3),
-               "api": "vd_forward (C ABI), pinned host inputs and outputs"}
-        if np.max(np.abs(out - got)) != 0.0:
+               "api": "vd_forward (C ABI), pinned host inputs and outputs" +
+                      ("; each rank writes its slices of a node-wide shared-memory output array" if world > 1 else "")}
+        if not np.array_equal(out, got):
             raise SystemExit("vd_forward and the resident plan disagree")
+        if shared_out is not None:
+            if rank == 0:
+                full_got = shared_out.values.copy()
+                o = _region_offsets(w)
+                for r in range(world):  # every rank's slices arrived, in input order
+                    if not np.all(np.isfinite(full_got[np.concatenate([np.arange(o[g], o[g + 1])
+                                                                       for g in shards[r]])]) |
+                                  np.isneginf(full_got[np.concatenate([np.arange(o[g], o[g + 1])
+                                                                       for g in shards[r]])])):
+                        raise SystemExit(f"rank {r}'s slices of the shared output are missing")
+            barrier()
+            shared_out.close()
 
-    # ---- CPU baseline (reference code, rank 0 at N=1) ----
+    # ---- the Python pair-list drop-in (score_pairs signature) on a >= 1e6-pair sample ----
+    e2e_pairs = None
+    if rank == 0 and world == 1 and not args.no_e2e:
+        from vardepth_b200.accelerator import CudaPairHMM
+        order = np.random.default_rng(99).permutation(w.n_regions)
+        npairs = np.diff(w.region_read_off) * np.diff(w.region_hap_off)
+        k = min(w.n_regions, int(np.searchsorted(np.cumsum(npairs[order]), 1_000_000)) + 1)
+        sample = np.sort(order[:k])
+        plist = _pair_list(w, sample)
+        scorer = CudaPairHMM(device=local, memory_mb=65536, gap=w.gap, ext=w.ext)
+        pl_cells = native.PairList(plist).cells()
+        for _ in range(warm):
+            res = scorer.score(plist)
+        ms = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res = scorer.score(plist)
+            ms.append(1e3 * (time.perf_counter() - t0))
+        o = _region_offsets(w)
+        if not np.array_equal(res, got[np.concatenate([np.arange(o[g], o[g + 1]) for g in sample])]):
+            raise SystemExit("score_pairs and the region batch disagree")
+        last = scorer.last
+        e2e_pairs = {"value": round(pl_cells / (np.mean(ms) / 1e3) / 1e9, 3), "unit": "GCUPS",
+                     "pairs": len(plist), "cells": int(pl_cells), "regions": int(k),
+                     "ms_per_step": round(float(np.mean(ms)), 3),
+                     "host_ms_per_step": round(1e3 * last["host_packing_seconds"], 3),
+                     "kernel_ms_per_step": round(1e3 * last["kernel_seconds"], 3),
+                     "h2d_bytes_per_step": int(last["h2d_bytes"]), "d2h_bytes_per_step": int(last["d2h_bytes"]),
+                     "api": "CudaPairHMM.score(list of (read str, quality bytes, haplotype str)): the list walked "
+                            "in C, validated, deduplicated and regrouped into regions by vd_score_pair_list"}
+        scorer.engine.close()
+
+    # ---- CPU baseline (reference code, rank 0 at N=1) and parity against it and the oracle ----
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        res = cpu_reference(w, args.cpu_seconds)
-        cpu = {"value": round(res["cells"] / res["times"][0] / 1e9, 4), "unit": "GCUPS", "cores": res["threads"],
-               "kind": "reference", "sample": res["sample"]}
+    parity = None
+    if rank == 0 and world == 1:
+        res = None
+        if not args.no_cpu:
+            res = cpu_reference(w, args.cpu_seconds)
+            cpu = {"value": round(res["cells"] / res["times"][0] / 1e9, 4), "unit": "GCUPS", "cores": res["threads"],
+                   "kind": "reference", "sample": res["sample"]}
+        parity = {}
+        region_cells = shard.region_cells(full)
+        if res is not None:
+            ref_out = np.concatenate([j[6] for j in res["jobs"]])
+            parity["vs_reference"] = dict(_compare(w, got, res["regions"], ref_out, region_cells),
+                                          checker="the reference's read_haplotype_batch_mode (oracle/_ref, "
+                                                  "compiled from wide.cpp), the CPU-baseline sample")
+            base_order = res["regions"]
+        else:
+            base_order = np.random.default_rng(12345).permutation(w.n_regions)
+        # the FP64 oracle on a prefix of the same seeded region order holding >= 1e10 cells
+        cum = np.cumsum(region_cells[base_order])
+        k = min(len(base_order), int(np.searchsorted(cum, 1e10)) + 1)
+        t0 = time.perf_counter()
+        parity["vs_oracle"] = dict(_compare(w, got, base_order[:k], _oracle(w, base_order[:k]), region_cells),
+                                   checker="FP64 restatement (oracle/)",
+                                   seconds=round(time.perf_counter() - t0, 1))
+        if args.workload == "mixed_length_regions":
+            # 20 regions of 1-10 kb reads (the drift and FP64 tiers' pairs), from the smaller half of them
+            rl = np.diff(w.read_off)
+            longest = np.maximum.reduceat(rl, w.region_read_off[:-1]) if len(rl) else rl
+            long_regions = np.flatnonzero(longest > 256)
+            small = long_regions[np.argsort(region_cells[long_regions])][:max(20, len(long_regions) // 2)]
+            pick = np.sort(np.random.default_rng(11).choice(small, size=min(20, len(small)), replace=False))
+            t0 = time.perf_counter()
+            parity["long_read"] = dict(_compare(w, got, pick, _oracle(w, pick), region_cells),
+                                       checker="FP64 restatement (oracle/)",
+                                       selection="20 seeded regions with 1-10 kb reads at 8% error, from the half "
+                                                 "with fewer cells", seconds=round(time.perf_counter() - t0, 1))
 
     primary_ms = allmax(primary_ms) / args.steps
     # batched regions: the primary tier holds all but ~0.5% of the work; elsewhere
@@ -542,38 +678,40 @@ def main():
     roof_ms = primary_ms if args.workload == "batched_regions" else step_ms
     # the FMA pipe only sees the cells it computes: columns a haplotype shares
     # with the previous one of its region are counted in value, not here
-    computed = cells - shared
+    computed = my_cells - shared
     achieved = computed * FLOPS_PER_CELL / (roof_ms / 1e3) / 1e12
-    traffic = None
+    traffic, traffic_source = None, None
     tf = ROOT / "profiles" / "pairhmm_f32_traffic.json"
-    if tf.exists() and args.workload == "batched_regions":
+    if tf.exists() and args.workload == "batched_regions" and world == 1:
         try:
             t = json.loads(tf.read_text())
             traffic = t.get("bytes_per_launch_full_batched_regions")
+            traffic_source = t.get("source")
         except (OSError, ValueError):
             traffic = None
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": max(3, args.warmup), "ms_per_step": round(step_ms, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "warmup": warm, "ms_per_step": round(step_ms, 3), "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload], "regions": args.regions, "pairs": pairs, "cells": cells,
-                       "shared_prefix_cells": int(shared), "seed": w.meta.get("seed"),
+                       "shared_prefix_cells": int(shared) if world == 1 else None, "seed": w.meta.get("seed"),
                        "inputs_bytes": w.input_bytes(), "l2": "inputs (%.2f GB) exceed the 126 MB L2; "
                        "the recurrence state lives in registers" % (w.input_bytes() / 1e9),
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "parallelism": f"{world} GPUs, LPT region shards" if world > 1 else "1 GPU",
                        "precision": "FP32 scaled, FP32 drift and FP64 rescue", "gpu": info["gpu"]},
             "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak.value, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / peak.value, 4), "traffic": traffic,
+                         "traffic_source": traffic_source,
                          "flops_per_cell": FLOPS_PER_CELL, "cells_computed": int(computed),
                          "kernel": "FP32 tier: pairhmm_pair_kernel x2 + pairhmm_kernel<float>"
                          if args.workload == "batched_regions" else "every tier (whole step)",
                          "primary_ms": round(primary_ms, 3),
                          "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
                          "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},
-            "plain": plain, "autotune": tuned,
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "rescued_pairs": int(rescued), "rescued_fraction": round(rescued / max(1, pairs), 6),
+            "plain": plain, "autotune": tuned, "sharding": sharding,
+            "cpu_baseline": cpu, "e2e": e2e, "e2e_pairs": e2e_pairs, "gpu_launches": launches,
+            "rescued_pairs": int(rescued), "rescued_fraction": round(rescued / max(1, mine.n_outputs()), 6),
             "rescued_fp32_drift_pairs": int(drift_rescued), "parity": parity, "clocks": sampler.summary(),
         }
         print(json.dumps(line), flush=True)

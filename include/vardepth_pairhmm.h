@@ -200,6 +200,34 @@ double vd_read_haplotype(const char *read, const unsigned char *qual, int n, con
 double vd_anchored_pairhmm(const char *read, const unsigned char *qual, int n, const char *hap,
                            int m, double gap, double ext);
 
+/* ---- the Python pair-list drop-in -----------------------------------------
+ * caller/native/caller/accelerator.py:166-186 score_pairs and :105-159
+ * CudaPairHMM.score take a list of (read, qualities, haplotype) triples; the
+ * Python layer of this library hands it over as the pointer arrays of the
+ * batch_hmm.cpp:192 convention (read, quality and haplotype pointers, read and
+ * haplotype lengths, one entry per pair), and this call does the rest of the
+ * host work natively: every distinct read and haplotype is checked for
+ * uppercase ACGTN (VD_EINVAL, "Uppercase DNA required", accelerator.py:31-33),
+ * identical reads (bases and qualities) and haplotypes are stored once,
+ * repeated pairs are scored once, and reads that ask for the same set of
+ * haplotypes are regrouped into one region, so the batch reaches the packed
+ * two-read kernels and the shared-prefix schedule.  out[p] (count doubles)
+ * receives pair p's ln L; empty reads or haplotypes give -inf.  The pointers
+ * are only read during the call. */
+int vd_score_pair_list(vd_engine *engine, const char *const *reads, const unsigned char *const *quals,
+                       const int *rn, const char *const *haps, const int *hn, int64_t count,
+                       const vd_params *params, double *out, vd_stats *stats);
+/* The regrouping vd_score_pair_list applies, on the host only (no device is
+ * used; no counterpart in the reference).  counts[4] receives the distinct
+ * reads, distinct haplotypes, regions and output slots of the region batch;
+ * the nullable per-pair arrays receive the distinct read id, haplotype id
+ * (both in order of first appearance), region (regions in order of their
+ * first read) and the pair's slot in the region batch's output (regions in
+ * order, each a reads x haplotypes row-major block, haplotypes in id order). */
+int vd_pair_list_plan(const char *const *reads, const unsigned char *const *quals, const int *rn,
+                      const char *const *haps, const int *hn, int64_t count, int64_t *counts,
+                      int32_t *pair_read, int32_t *pair_hap, int32_t *pair_region, int64_t *pair_slot);
+
 /* ---- gradient --------------------------------------------------------------
  * No counterpart in the reference (it has no differentiable PairHMM).  For the
  * semiglobal model, every pair's ln L and its six partial derivatives

@@ -225,6 +225,36 @@ def test_pairs_regions_and_chunking_agree():
     np.testing.assert_array_equal(chunked_pairs, regions)
 
 
+def test_pair_list_regrouping_gives_the_region_results():
+    """score() on a pair list (validated, deduplicated and regrouped into regions in native
+    code) gives the region form's results bit for bit, in any pair order, with repeated pairs
+    and reads passed as different objects of equal content."""
+    w = S.batched_regions(n_regions=60)
+    eng = CudaPairHMM(memory_mb=4096, gap=w.gap, ext=w.ext)
+    want = eng.score_packed(_packed(w))
+    pairs, idx = [], []
+    o = 0
+    for g in range(w.n_regions):
+        haps = [bytes(w.hap_bases[w.hap_off[h]:w.hap_off[h + 1]]).decode()
+                for h in range(w.region_hap_off[g], w.region_hap_off[g + 1])]
+        for r in range(w.region_read_off[g], w.region_read_off[g + 1]):
+            a, b = w.read_off[r], w.read_off[r + 1]
+            s = bytes(w.read_bases[a:b]).decode()
+            q = bytes(w.read_quals[a:b]) if r % 2 else w.read_quals[a:b].tolist()
+            for h in haps:
+                pairs.append((s, q, h))
+                idx.append(o)
+                o += 1
+    rng = np.random.default_rng(3)
+    extra = rng.integers(0, len(pairs), 500)
+    pairs += [(pairs[i][0][:], bytes(np.asarray(pairs[i][1], np.uint8)), pairs[i][2]) for i in extra]
+    idx += [idx[i] for i in extra]
+    perm = rng.permutation(len(pairs))
+    got = eng.score([pairs[i] for i in perm])
+    np.testing.assert_array_equal(got, want[np.asarray(idx)[perm]])
+    assert eng.last["pairs"] == len(pairs)
+
+
 def test_pipelined_chunks_agree():
     """vd_forward's pipelined chunks (the first a quarter of the others, each chunk's
     primary tier ordered after the previous one's) give the single-chunk results bit for bit."""

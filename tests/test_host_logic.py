@@ -217,3 +217,76 @@ def test_drift_boosts_cancel_exactly():
         want = O.forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10)
         assert abs(boosted - plain) <= 1e-12 * abs(plain)
         assert abs(plain - want) <= 1e-9 * abs(want)
+
+
+def _pair_list_mirror(pairs):
+    """The regrouping of vd_score_pair_list restated: distinct reads (bases, qualities) and
+    haplotypes numbered in order of first appearance; reads asking for the same set of
+    haplotypes form a region (regions in order of their first read); a pair's slot is its
+    (read, haplotype) cell of its region's reads x haplotypes block, haplotypes in id order."""
+    rid, hid, rlist = {}, {}, []
+    pr, ph = [], []
+    for s, q, h in pairs:
+        rk = (s, q if isinstance(q, bytes) else bytes(np.asarray(q).astype(np.uint8)))
+        pr.append(rid.setdefault(rk, len(rid)))
+        ph.append(hid.setdefault(h, len(hid)))
+    sets = [set() for _ in rid]
+    for r, h in zip(pr, ph):
+        sets[r].add(h)
+    region_of, members, hapsets = {}, [], []
+    read_region = []
+    for r, hs in enumerate(sets):
+        key = tuple(sorted(hs))
+        if key not in region_of:
+            region_of[key] = len(members)
+            members.append([])
+            hapsets.append(list(key))
+        read_region.append(region_of[key])
+        members[region_of[key]].append(r)
+    off = np.concatenate([[0], np.cumsum([len(m) * len(hs) for m, hs in zip(members, hapsets)])])
+    slot = [off[read_region[r]] + members[read_region[r]].index(r) * len(hapsets[read_region[r]])
+            + hapsets[read_region[r]].index(h) for r, h in zip(pr, ph)]
+    return pr, ph, [read_region[r] for r in pr], slot, len(members), int(off[-1])
+
+
+def test_pair_list_plan_matches_its_restatement():
+    from vardepth_b200 import native
+    rng = np.random.default_rng(5)
+    haps = ["".join(rng.choice(list("ACGT"), int(rng.integers(1, 40)))) for _ in range(9)] + [""]
+    regions = [rng.choice(len(haps), size=int(rng.integers(1, 5)), replace=False) for _ in range(6)]
+    pairs = []
+    for g, hs in enumerate(regions):
+        for _ in range(int(rng.integers(1, 6))):
+            n = int(rng.integers(0, 12))
+            s = "".join(rng.choice(list("ACGTN"), n))
+            q = rng.integers(0, 61, n)
+            # the same qualities as bytes, a list, a tuple or a numpy array of another dtype
+            q = [bytes(q.astype(np.uint8)), q.tolist(), tuple(int(x) for x in q), q.astype(np.int64)][g % 4]
+            for h in hs:
+                pairs.append((s, q, haps[h]))
+    pairs += pairs[3:7]                                   # repeated pairs
+    pairs.append((pairs[0][0][:], list(pairs[0][1]), pairs[0][2]))  # equal content, other objects
+    order = rng.permutation(len(pairs))
+    pairs = [pairs[i] for i in order]
+    got = native.pair_list_plan(pairs)
+    pr, ph, preg, slot, ng, nslots = _pair_list_mirror(pairs)
+    assert list(got["read"]) == pr and list(got["hap"]) == ph
+    assert list(got["region"]) == preg and list(got["slot"]) == slot
+    assert got["n_regions"] == ng and got["n_slots"] == nslots
+
+
+def test_pair_list_validation_messages():
+    from vardepth_b200 import native
+    cases = [([("ACGT", [30, 30, 30], "A")], "Read/quality lengths differ"),
+             ([("ACGT", [30, 30, 30, 256], "A")], "integer Phred"),
+             ([("ACGT", [30, 30, 30, 2.5], "A")], "integer Phred"),
+             ([("ACGT", np.array([[30, 30], [30, 30]]), "A")], "integer Phred"),
+             ([("acgt", [30] * 4, "A")], "Uppercase DNA required"),
+             ([("ACGT", [30] * 4, "AXA")], "Uppercase DNA required"),
+             ([(b"ACGT", [30] * 4, "A")], "Uppercase DNA required"),
+             ([("ACGTé", [30] * 5, "A")], "Uppercase DNA required")]
+    for pairs, msg in cases:
+        with pytest.raises(ValueError, match=msg):
+            native.pair_list_plan(pairs)
+    ok = native.pair_list_plan([("ACGTN", b"\x00\x01\x3c\xff\x1e", "N"), ("", b"", "ACGT"), ("A", [0], "")])
+    assert ok["n_reads"] == 3 and ok["n_haps"] == 3

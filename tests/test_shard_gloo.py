@@ -1,6 +1,7 @@
 """The multi-GPU path on the CPU: regions sharded over world_size 2 gloo ranks (127.0.0.1),
-each rank scoring its own shard (here with the oracle as a stand-in scorer: no GPU), and one
-gather reassembling the full output vector on rank 0 in the batch's output order."""
+each rank scoring its own shard (here with the oracle as a stand-in scorer: no GPU), and the
+full output vector reassembled on rank 0 in the batch's output order, through the node's
+shared-memory array (each rank writes its slices) or through one gather."""
 import os
 import socket
 
@@ -28,13 +29,13 @@ def _oracle_scorer(gap, ext):
     return score
 
 
-def _rank(rank, world, port, result_path):
+def _rank(rank, world, port, result_path, shared_name):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import datetime
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         w, packed = _workload()
-        full = shard.score_sharded(packed, rank, world, _oracle_scorer(w.gap, w.ext))
+        full = shard.score_sharded(packed, rank, world, _oracle_scorer(w.gap, w.ext), shared_name=shared_name)
         if rank == 0:
             np.save(result_path, full)
         else:
@@ -67,10 +68,14 @@ def test_subset_positions_cover_the_outputs():
     assert sum(sub.n_outputs() for sub, _ in parts) == packed.n_outputs()
 
 
-def test_two_gloo_ranks_reassemble_the_batch(tmp_path):
+@pytest.mark.parametrize("shared", [True, False])
+def test_two_gloo_ranks_reassemble_the_batch(tmp_path, shared):
     w, packed = _workload()
     result = tmp_path / "full.npy"
-    mp.start_processes(_rank, args=(2, _free_port(), str(result)), nprocs=2, join=True, start_method="spawn")
+    name = f"vd_test_{os.getpid()}" if shared else None
+    mp.start_processes(_rank, args=(2, _free_port(), str(result), name), nprocs=2, join=True, start_method="spawn")
     full = np.load(result)
     want = _oracle_scorer(w.gap, w.ext)(packed)
     np.testing.assert_array_equal(full, want)
+    if shared:
+        assert not os.path.exists(f"/dev/shm/{name}")  # rank 0 removed the segment

@@ -34,7 +34,6 @@ from . import native
 HERE = Path(__file__).resolve().parent
 _ENGINE = None
 _ENGINE_KEY = None
-_DNA = frozenset("ACGTN")
 
 DEFAULT_GAP = 0.001   # every production call site (accelerator.py:52, base/caller.py:140)
 DEFAULT_EXT = 0.1
@@ -43,42 +42,30 @@ DEFAULT_EXT = 0.1
 def validate_pairs(pairs):
     """Check (read, qualities, haplotype) triples; return them with uint8 qualities.
 
-    Same rules and messages as accelerator.py:25-40: read and quality lengths
+    Same rules and messages as accelerator.py:25-40 (read and quality lengths
     agree, sequences are uppercase ACGTN strings, qualities are integer Phred
-    scores in [0, 255].
+    scores in [0, 255]), checked in native code: the pair list is walked once
+    by ``_pairlist.gather`` and the bases by ``vd_pair_list_plan``.
     """
-    result = []
-    seen_dna = set()
-    seen_q = {}
-    for sequence, qualities, haplotype in pairs:
-        if len(sequence) != len(qualities):
-            raise ValueError("Read/quality lengths differ")
-        for dna in (sequence, haplotype):
-            if dna not in seen_dna:
-                if not isinstance(dna, str) or not set(dna) <= _DNA:
-                    raise ValueError("Uppercase DNA required")
-                seen_dna.add(dna)
-        key = id(qualities)
-        if key not in seen_q:
-            q = np.frombuffer(qualities, np.uint8) if isinstance(qualities, (bytes, bytearray)) else np.asarray(qualities)
-            if q.ndim != 1:
-                raise ValueError("Base qualities must be integer Phred scores in [0,255]")
-            if q.size:
-                qf = q.astype(np.float64, copy=False)
-                if (not np.all(np.isfinite(qf)) or np.any(qf < 0) or np.any(qf > 255)
-                        or np.any(qf != np.floor(qf))):
-                    raise ValueError("Base qualities must be integer Phred scores in [0,255]")
-            # keep the object alive so its id cannot be recycled while cached
-            seen_q[key] = (qualities, np.ascontiguousarray(q, dtype=np.uint8))
-        result.append((sequence, seen_q[key][1], haplotype))
-    return result
+    pairs = list(pairs)
+    gathered = native.PairList(pairs)      # types, Phred range, lengths
+    native.pair_list_plan(gathered)        # ACGTN of every distinct read and haplotype
+    # one uint8 array per distinct quality object (``pairs`` keeps the objects, and so their
+    # ids, alive while the table is used)
+    arrays = {}
+    for _, q, _ in pairs:
+        if id(q) not in arrays:
+            arrays[id(q)] = np.frombuffer(q, np.uint8) if isinstance(q, bytes) else np.asarray(q).astype(np.uint8)
+    return [(s, arrays[id(q)], h) for s, q, h in pairs]
 
 
 def pack_pairs(pairs) -> native.Packed:
     """Pack validated pairs into the pair form of vd_batch.
 
     Identical reads (same bases and qualities) and identical haplotypes are
-    stored once; out[p] belongs to pairs[p].
+    stored once; out[p] belongs to pairs[p].  (CudaPairHMM.score does this in
+    native code through vd_score_pair_list; this form is for callers that
+    want the packed batch itself.)
     """
     reads: dict = {}
     haps: dict = {}
@@ -87,7 +74,7 @@ def pack_pairs(pairs) -> native.Packed:
     pr = np.empty(len(pairs), np.int32)
     ph = np.empty(len(pairs), np.int32)
     for p, (s, q, h) in enumerate(pairs):
-        key = (s, q.tobytes())
+        key = (s, np.asarray(q, np.uint8).tobytes())
         r = reads.get(key)
         if r is None:
             r = len(reads)
@@ -150,13 +137,14 @@ class CudaPairHMM:
         return native.make_params(self.gap, self.ext, anchored, mode, quality_offsets)
 
     def score(self, pairs, anchored=False):
+        """ln L of (read, qualities, haplotype) triples in input order.  The list is walked
+        once in C (pointers into the Python objects, no copies) and validated, deduplicated
+        and regrouped into regions in the library (vd_score_pair_list)."""
         start = time.perf_counter()
-        pairs = validate_pairs(pairs)
-        pack_start = time.perf_counter()
-        packed = pack_pairs(pairs)
-        packing = time.perf_counter() - pack_start
+        gathered = native.PairList(pairs)
+        packing = time.perf_counter() - start
         params, _keep = self._params(anchored)
-        out, st = self.engine.forward(packed, params)
+        out, st = self.engine.score_pair_list(gathered, params)
         self._record(st, anchored, start, packing)
         return out
 
@@ -241,9 +229,8 @@ def score_many(sequences, qualities, haplotypes, selection=None):
     _choose(selection)
     if not len(sequences) or not len(haplotypes):
         return np.empty((len(sequences), len(haplotypes)), np.float64)
-    pairs = validate_pairs([(s, q, haplotypes[0]) for s, q in zip(sequences, qualities)])
-    for h in haplotypes:
-        validate_pairs([("", b"", h)])
+    pairs = validate_pairs([(s, q, h) for s, q in zip(sequences, qualities) for h in haplotypes[:1]] +
+                           [("", b"", h) for h in haplotypes])[:len(sequences)]
     rb = b"".join(s.encode("ascii") for s, _, _ in pairs)
     rq = b"".join(q.tobytes() for _, q, _ in pairs)
     roff = np.concatenate([[0], np.cumsum([len(s) for s, _, _ in pairs])]).astype(np.int64)

@@ -37,6 +37,7 @@ UNITS = [
     ("noalloc", "pairhmm_noalloc.cu", []),
     ("grad", "pairhmm_grad.cu", []),
     ("genotype", "pairhmm_genotype.cu", []),
+    ("pairlist", "pairhmm_pairlist.cu", []),
 ]
 
 
@@ -69,8 +70,28 @@ def _compile(unit, log):
     return out
 
 
+def build_pairlist(force: bool = False) -> Path:
+    """The CPython helper of the pair-list drop-in (csrc/pairlist_py.c -> _pairlist*.so)."""
+    import sysconfig
+    out = HERE / ("_pairlist" + sysconfig.get_config_var("EXT_SUFFIX"))
+    src = CSRC / "pairlist_py.c"
+    if not force and out.exists() and out.stat().st_mtime >= src.stat().st_mtime:
+        return out
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        raise RuntimeError("a C compiler is required to build vardepth_b200._pairlist")
+    tmp = out.with_name(out.name + f".{os.getpid()}.tmp")
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-Wall", f"-I{sysconfig.get_paths()['include']}", str(src), "-o", str(tmp)]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"building _pairlist failed:\n{proc.stderr[-4000:]}")
+    tmp.replace(out)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     """Compile (if needed) and return the path of the shared library."""
+    build_pairlist(force)
     stamp = HERE / "libvardepth_pairhmm.sha256"
     fp = _fingerprint()
     if not force and LIB.exists() and stamp.exists() and stamp.read_text().strip() == fp:

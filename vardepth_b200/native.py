@@ -117,6 +117,12 @@ SIGNATURES = {
     "vd_forward_region_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  c_i64, ctypes.c_void_p, ctypes.c_void_p, c_i64,
                                                  ctypes.POINTER(VdParams), ctypes.c_void_p, ctypes.c_void_p]),
+    # pointer arrays of the Python pair list (vardepth_b200._pairlist.gather)
+    "vd_score_pair_list": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, c_i64, ctypes.POINTER(VdParams), c_dp,
+                                          ctypes.POINTER(VdStats)]),
+    "vd_pair_list_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, c_i64, c_i64p, c_i32p, c_i32p, c_i32p, c_i64p]),
     "vd_last_error": (ctypes.c_char_p, []),
     "vd_device_count": (ctypes.c_int, []),
     "vd_version": (ctypes.c_char_p, []),
@@ -226,6 +232,45 @@ def prefix_plan(hap_bases: np.ndarray, hap_off: np.ndarray):
     return order, share
 
 
+class PairList:
+    """A Python list of (read, qualities, haplotype) triples as the pointer arrays of the
+    reference's pair-list calling convention (batch_hmm.cpp:192), pointing into the Python
+    objects themselves (vardepth_b200._pairlist.gather).  Raises ValueError with the
+    reference's messages for reads or haplotypes that are not ASCII str, qualities that are
+    not integer Phred scores in [0, 255], and read/quality length mismatches; the ACGTN check
+    runs in the library."""
+
+    def __init__(self, pairs):
+        try:
+            from . import _pairlist
+        except ImportError as e:  # the helper is built with the library
+            raise RuntimeError("vardepth_b200._pairlist is not built: run `python -m vardepth_b200.build`") from e
+        self.pairs = pairs if isinstance(pairs, (list, tuple)) else list(pairs)
+        (self.count, self._reads, self._quals, self._rn, self._haps, self._hn,
+         self._keep) = _pairlist.gather(self.pairs)
+        addr = lambda b: np.frombuffer(b, np.uint8).ctypes.data if len(b) else None
+        self.args = tuple(addr(b) for b in (self._reads, self._quals, self._rn, self._haps, self._hn))
+
+    def cells(self) -> int:
+        return int(np.dot(np.frombuffer(self._rn, np.int32).astype(np.int64),
+                          np.frombuffer(self._hn, np.int32).astype(np.int64)))
+
+
+def pair_list_plan(pairs) -> dict:
+    """The regrouping vd_score_pair_list applies to a pair list (vd_pair_list_plan; host only)."""
+    pl = pairs if isinstance(pairs, PairList) else PairList(pairs)
+    n = pl.count
+    counts = np.zeros(4, np.int64)
+    out = {k: np.empty(n, dt) for k, dt in (("read", np.int32), ("hap", np.int32), ("region", np.int32),
+                                               ("slot", np.int64))}
+    check(library().vd_pair_list_plan(*pl.args, n, counts.ctypes.data_as(c_i64p),
+                                      out["read"].ctypes.data_as(c_i32p), out["hap"].ctypes.data_as(c_i32p),
+                                      out["region"].ctypes.data_as(c_i32p), out["slot"].ctypes.data_as(c_i64p)),
+          "vd_pair_list_plan")
+    out.update(n_reads=int(counts[0]), n_haps=int(counts[1]), n_regions=int(counts[2]), n_slots=int(counts[3]))
+    return out
+
+
 def make_params(gap: float, ext: float, anchored: bool, precision: int, quality_offsets=None,
                 schedule: int = VD_SCHEDULE_BATCHED):
     p = VdParams()
@@ -285,6 +330,17 @@ class Engine:
         stats = VdStats()
         check(library().vd_forward(self.handle, ctypes.byref(packed.batch), ctypes.byref(params),
                                    out.ctypes.data_as(c_dp), ctypes.byref(stats)), "vd_forward")
+        return out, stats
+
+    def score_pair_list(self, pairs, params: VdParams, out: np.ndarray | None = None):
+        """ln L of a list of (read, qualities, haplotype) triples in input order, through
+        vd_score_pair_list (validation, dedupe and regrouping into regions in native code)."""
+        pl = pairs if isinstance(pairs, PairList) else PairList(pairs)
+        if out is None:
+            out = np.empty(pl.count, np.float64)
+        stats = VdStats()
+        check(library().vd_score_pair_list(self.handle, *pl.args, pl.count, ctypes.byref(params),
+                                           out.ctypes.data_as(c_dp), ctypes.byref(stats)), "vd_score_pair_list")
         return out, stats
 
     def forward_backward(self, packed: Packed, params: VdParams, checkpoint: int = VD_CHECKPOINT_SQRT):

@@ -4,8 +4,11 @@ Regions are independent, so each rank scores a disjoint set of regions on its
 own GPU with its own persistent queue, and the results land in disjoint
 slices of the full output vector.  Regions go to ranks longest-processing-time
 first by DP cells (sum of n*m over the region's pairs), which balances the
-ranks' kernel time.  Only when one rank must hold every result does a single
-gather run at the end (torch.distributed: NCCL between GPUs, gloo on CPUs).
+ranks' kernel time.  On one node the full output vector is a shared-memory
+array that every rank writes its slices of (``SharedOutput``), so rank 0 holds
+every result after one barrier and no result crosses a collective; across
+nodes a single gather at the end collects them (torch.distributed: NCCL
+between GPUs, gloo on CPUs).
 """
 from __future__ import annotations
 
@@ -67,24 +70,71 @@ def subset(packed: native.Packed, regions: np.ndarray):
     return sub, cat(pos, np.int64)
 
 
-def score_sharded(packed: native.Packed, rank: int, world: int, scorer, gather: bool = True, group=None):
+class SharedOutput:
+    """The full output vector (float64) in POSIX shared memory, one per node: each rank
+    writes the slices of its regions and rank 0 reads the whole vector after a barrier.
+    Rank 0 creates the segment (``name``) before the others attach."""
+
+    def __init__(self, name: str, n: int, create: bool):
+        from multiprocessing import resource_tracker, shared_memory
+        size = max(8, 8 * int(n))
+        if create:
+            try:  # a segment left by an earlier run under the same name
+                old = shared_memory.SharedMemory(name=name)
+                old.close()
+                old.unlink()
+            except FileNotFoundError:
+                pass
+            self.shm = shared_memory.SharedMemory(name=name, create=True, size=size)
+        else:
+            self.shm = shared_memory.SharedMemory(name=name)
+            # the creator unlinks it; this rank's resource tracker must not
+            resource_tracker.unregister(self.shm._name, "shared_memory")
+        self.creator = create
+        self.values = np.ndarray((int(n),), np.float64, buffer=self.shm.buf)
+
+    def write(self, positions: np.ndarray, values: np.ndarray) -> None:
+        self.values[positions] = values
+
+    def close(self) -> None:
+        self.values = None
+        self.shm.close()
+        if self.creator:
+            self.shm.unlink()
+
+
+def score_sharded(packed: native.Packed, rank: int, world: int, scorer, gather: bool = True, group=None,
+                  shared_name: str | None = None):
     """Score this rank's shard with ``scorer(sub_packed) -> ln L`` (normally
     ``lambda p: engine.forward(p, params)[0]`` on this rank's GPU).
 
-    Returns (positions, values) of this rank's outputs; with gather=True rank 0
-    instead receives the full output vector (other ranks get None) through one
-    torch.distributed gather_object at the end.
+    Returns (positions, values) of this rank's outputs.  With gather=True rank 0 instead
+    receives the full output vector (other ranks get None): through the node's shared-memory
+    array when ``shared_name`` is given (every rank writes its slices, then one barrier), else
+    through one torch.distributed gather_object at the end (ranks on several nodes).
     """
     shards = shard_regions(region_cells(packed), world)
     sub, pos = subset(packed, shards[rank])
     values = np.asarray(scorer(sub), np.float64) if len(pos) else np.empty(0)
-    if not gather or world == 1:
-        if world == 1 and gather:
-            full = np.empty(packed.n_outputs())
-            full[pos] = values
-            return full
+    if not gather:
         return pos, values
+    if world == 1:
+        full = np.empty(packed.n_outputs())
+        full[pos] = values
+        return full
     import torch.distributed as dist
+    if shared_name is not None:
+        if rank == 0:
+            out = SharedOutput(shared_name, packed.n_outputs(), create=True)
+        dist.barrier(group=group)          # the segment exists
+        if rank != 0:
+            out = SharedOutput(shared_name, packed.n_outputs(), create=False)
+        out.write(pos, values)
+        dist.barrier(group=group)          # every slice is written
+        full = out.values.copy() if rank == 0 else None
+        dist.barrier(group=group)          # rank 0 has read it
+        out.close()
+        return full
     parts = [None] * world if rank == 0 else None
     dist.gather_object((pos, values), parts, dst=0, group=group)
     if rank != 0:
