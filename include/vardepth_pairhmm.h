@@ -128,7 +128,8 @@ int vd_engine_info(const vd_engine *engine, char *name, int name_len, int *major
  * on (the autotuner in vardepth_b200/autotune.py measures and sets them).
  * No counterpart in the reference. */
 typedef struct vd_tuning {
-  int long_read_rows;   /* strip height of reads longer than 256 bases: 64, 128 or 256 (default);
+  int long_read_rows;   /* strip height of reads longer than 256 bases: 64, 128 or 256 (default;
+                           VD_LONG_WARP runs 128 or 256);
                            shorter strips are renormalised more often, so error-rich long reads
                            stay in the FP32 tier */
   int pair_mask;        /* bit R (1..8): two reads with R rows per lane may share a warp in the
@@ -138,8 +139,13 @@ typedef struct vd_tuning {
                            min(8, N / this) chunks (the first a quarter of the others), so the
                            host work and copies of one chunk overlap the kernels of the previous
                            one; 0 = the default (300), 1e6 or more = one chunk */
-  int reserved[4];      /* must be zero */
+  int long_mode;        /* reads longer than one strip, FP32 semiglobal: VD_LONG_WARP (default) runs a
+                           read against two haplotypes per warp with per-lane power-of-two boosts;
+                           VD_LONG_SINGLE runs them in the single-read kernel (strips renormalised
+                           exactly, error-rich reads then rescued by the drift tier) */
+  int reserved[3];      /* must be zero */
 } vd_tuning;
+enum { VD_LONG_WARP = 0, VD_LONG_SINGLE = 1 };
 int vd_engine_set_tuning(vd_engine *engine, const vd_tuning *tuning);
 int vd_engine_get_tuning(const vd_engine *engine, vd_tuning *tuning);
 

@@ -247,7 +247,8 @@ def test_pair_list_regrouping_gives_the_region_results():
                 o += 1
     rng = np.random.default_rng(3)
     extra = rng.integers(0, len(pairs), 500)
-    pairs += [(pairs[i][0][:], bytes(np.asarray(pairs[i][1], np.uint8)), pairs[i][2]) for i in extra]
+    as_bytes = lambda q: q if isinstance(q, bytes) else bytes(np.asarray(q).astype(np.uint8))
+    pairs += [(pairs[i][0][:], as_bytes(pairs[i][1]), pairs[i][2]) for i in extra]
     idx += [idx[i] for i in extra]
     perm = rng.permutation(len(pairs))
     got = eng.score([pairs[i] for i in perm])
@@ -519,10 +520,48 @@ def test_drift_tier_error_rich_long_reads():
         regions.append((haps, reads, quals))
     w = S._assemble("drift", regions, S.GAP_Q45, S.EXT_Q10, {})
     eng = native.Engine(0, 4096)
+    eng.set_tuning(long_mode=native.VD_LONG_SINGLE)  # long reads in the single-read kernel, then the drift tier
     batched, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
     plain, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED, schedule=native.VD_SCHEDULE_PLAIN)
     a, st = eng.forward(_packed(w), batched)
     assert st.rescued_fp32 >= 20 and st.rescued_fp64 + st.rescued_robust <= 2
     assert_mixed_close(a, _oracle_workload(w))
     np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], a)
+    eng.close()
+
+
+def _long_read_regions(seed, lengths, err, n_haps):
+    """One region per read length: n_haps haplotypes (a base and edited copies of unequal
+    lengths) and two reads of that length at substitution rate err (indels err / 4)."""
+    rng = np.random.default_rng(seed)
+    qf = S._q_standard(rng)
+    regions = []
+    for n in lengths:
+        hap0 = S._random_hap(rng, n + int(rng.integers(100, 600)))
+        haps = [hap0] + [S._mutate(rng, hap0, 3, int(rng.integers(1, 11))) for _ in range(n_haps - 1)]
+        reads, quals = S._sim_reads(rng, haps, 2, np.full(2, n), err, err / 4, qf)
+        regions.append((haps, reads, quals))
+    return S._assemble("long", regions, S.GAP_Q45, S.EXT_Q10, {"seed": seed})
+
+
+@pytest.mark.parametrize("err,n_haps", [(0.08, 3), (0.01, 4)])
+def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
+    """Reads of 257, 1,500 and 10,000 bases in the long-read kernel (one read against two
+    haplotypes per warp, per-lane power-of-two boosts): within 1e-4 log10 of the FP64 oracle
+    with no pair left to FP64 and the genotype argmax unchanged, bit-identical under the plain
+    schedule (one haplotype per warp) and with 128-row strips within the same bound."""
+    w = _long_read_regions(int(err * 1000) + n_haps, [257, 1500, 10000], err, n_haps)
+    want = _oracle_workload(w)
+    eng = native.Engine(0, 8192)
+    batched, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    plain, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED, schedule=native.VD_SCHEDULE_PLAIN)
+    got, st = eng.forward(_packed(w), batched)
+    assert_mixed_close(got, want)
+    assert st.rescued_fp64 + st.rescued_robust == 0 and st.rescued_fp32 == 0
+    assert _argmax_agree(w, got, want) == (w.n_regions, w.n_regions)
+    np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], got)
+    eng.set_tuning(long_read_rows=128)
+    assert_mixed_close(eng.forward(_packed(w), batched)[0], want)
+    eng.set_tuning(long_mode=native.VD_LONG_SINGLE)
+    assert_mixed_close(eng.forward(_packed(w), batched)[0], want)
     eng.close()

@@ -12,7 +12,11 @@ lays out the work list:
   packed FP32 kernel (fewer issue slots per cell, more registers per warp);
 * ``max_item_columns``  how many haplotype columns one work item streams
   (shorter items balance the tail of the persistent queue, longer ones pay
-  the 31-step wavefront ramp less often).
+  the 31-step wavefront ramp less often);
+* ``long_mode``  how reads longer than one strip run: two haplotypes of the
+  read per warp with per-lane power-of-two boosts (``VD_LONG_WARP``), or one
+  pair per warp in the single-read kernel with exact strip renormalisation
+  and the drift tier behind it (``VD_LONG_SINGLE``).
 
 ``autotune`` times candidate settings with resident plans (CUDA events around
 the captured tier graph) on a seeded region sample of the caller's batch,
@@ -29,8 +33,9 @@ import numpy as np
 
 from . import native
 
-DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0}
+DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0, "long_mode": native.VD_LONG_WARP}
 SPACE = {
+    "long_mode": [native.VD_LONG_WARP, native.VD_LONG_SINGLE],
     "long_read_rows": [256, 128, 64],
     "pair_mask": [0x1FE, 0x1F0, 0],
     "max_item_columns": [0, 16384, 4096],

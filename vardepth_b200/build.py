@@ -31,6 +31,7 @@ UNITS = [
     ("inst_f64_sg", "pairhmm_inst.cu", ["-DVD_FP64=1", "-DVD_ANCH=0"]),
     ("inst_f64_an", "pairhmm_inst.cu", ["-DVD_FP64=1", "-DVD_ANCH=1"]),
     ("drift", "pairhmm_drift.cu", []),
+    ("long", "pairhmm_long_inst.cu", []),
     ("launch", "pairhmm_launch.cu", []),
     ("host", "pairhmm_host.cu", []),
     ("peak", "pairhmm_peak.cu", []),

@@ -48,7 +48,7 @@ struct WorkItem {
   int32_t nhap;       // haplotypes in the list
   int64_t hap_begin;  // first haplotype (contiguous lists) or offset into hap_sel
   int64_t out_begin;  // output slot of the first haplotype, or offset into out_sel
-  int32_t code;       // R | general << 8 | multistrip << 9 | paired << 10
+  int32_t code;       // R | general << 8 | multistrip << 9 | paired << 10 | long << 11
   int32_t read2;      // second read of a paired item (same region and R), else -1
   int64_t out2_begin; // output slot of the second read's first haplotype
 };
@@ -67,6 +67,8 @@ inline __host__ __device__ int make_code(int R, bool general, bool multistrip) {
   return R | (general ? 256 : 0) | (multistrip ? 512 : 0);
 }
 constexpr int kPairedBit = 1024;
+constexpr int kLongBit = 2048;  // a long read against one or two haplotypes (pairhmm_long.cuh)
+inline __host__ __device__ bool code_long(int c) { return (c >> 11) & 1; }
 
 // Per-quality tables (index = raw Phred byte) and scalar constants for one
 // (gap, ext, offsets) setting, in the arithmetic type of the kernel.

@@ -184,8 +184,9 @@ struct vd_engine {
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair[2] = {0, 0};          // blocks of the two-read kernels [wide]
   int grid_drift = 0;                 // blocks of the drift tier (no more than grid[0][0])
+  int grid_long[2] = {0, 0};          // blocks of the long-read kernel [R == 8] (no more than grid[0][0])
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
-  vd_tuning tuning{256, 0x1fe, 0, 0, {0, 0, 0, 0}};  // vd_engine_set_tuning
+  vd_tuning tuning{256, 0x1fe, 0, 0, VD_LONG_WARP, {0, 0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
   DevBuf geno_arena;                  // buffers of vd_region_genotypes
   // table cache
@@ -299,6 +300,7 @@ int64_t batch_outputs(const vd_batch* b) {
 // Work-list choices the engine's tuning sets (vd_tuning).
 struct BuildOpts {
   int long_R = kMaxR;              // rows per lane of reads longer than one 256-row strip
+  bool long_warp = true;           // such reads (FP32 semiglobal) run two haplotypes per warp
   int pair_mask = 0x1fe;           // bit R: two reads of R rows per lane may share a warp
   int64_t max_stream = 1 << 30;    // haplotype columns one work item streams at most
 };
@@ -315,6 +317,7 @@ BuildOpts build_opts(const vd_engine* e) {
   bo.long_R = e->tuning.long_read_rows / kWarp;
   bo.pair_mask = e->tuning.pair_mask;
   bo.max_stream = e->tuning.max_item_columns > 0 ? (int64_t)e->tuning.max_item_columns : (int64_t)1 << 30;
+  bo.long_warp = e->tuning.long_mode == VD_LONG_WARP && (bo.long_R == 8 || bo.long_R == 4);
   return bo;
 }
 
@@ -345,6 +348,8 @@ struct HostChunk {
   bool any_strip = false;          // a read longer than one 256-row strip (every tier strip-mines it)
   int64_t n_paired = 0;            // leading items that carry two reads (own kernels)
   int64_t n_paired_wide = 0;       // the first of them, with 6-8 rows per lane
+  int64_t n_long = 0;              // the items after them: long reads, two haplotypes per warp
+  int long_R = kMaxR;              // rows per lane of those
 };
 
 // The robust tier runs on a small grid: it only sees pairs the FP64 wavefront
@@ -520,7 +525,9 @@ void region_order_and_shares(const vd_batch* b, int64_t h_lo, int64_t h_hi, int6
 void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSet* ts, bool offsets,
                         bool anchored, bool pair_reads, HostChunk& c, bool plain = false,
                         const BuildOpts& bo = BuildOpts()) {
+  const bool fp32 = pair_reads;  // mixed precision: the FP32 kernels run the primary tier
   if (plain) pair_reads = false;
+  c.long_R = bo.long_R;
   c.ra = b->region_read_off[g0];
   c.rb = b->region_read_off[g1];
   c.ha = b->region_hap_off[g0];
@@ -565,6 +572,33 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
     if (sharing)
       region_order_and_shares(b, h_lo, h_hi, c.ha, c.hap_order.data() + (h_lo - c.ha),
                               c.hap_share.data() + (h_lo - c.ha));
+    // a long read (FP32 semiglobal, one-sided emission) against its region's
+    // non-empty haplotypes, two neighbours per item (one in the plain schedule)
+    auto emit_long = [&](int64_t r) {
+      const int32_t code = c.read_code[r - c.ra];
+      const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
+      const int64_t rows = (int64_t)kWarp * bo.long_R * ((n + kWarp * bo.long_R - 1) / (kWarp * bo.long_R));
+      auto len = [&](int64_t h) { return (int)(b->hap_off[h + 1] - b->hap_off[h]); };
+      for (int64_t h = h_lo; h < h_hi;) {
+        const int m = len(h);
+        if (m <= 0) { ++h; continue; }
+        const bool two = !plain && h + 1 < h_hi && len(h + 1) > 0;
+        const int m2 = two ? len(h + 1) : 0;
+        WorkItem w;
+        w.read = (int32_t)(r - c.ra);
+        w.nhap = two ? 2 : 1;
+        w.hap_begin = h - c.ha;
+        w.out_begin = region_out + (r - r_lo) * nh + (h - h_lo);
+        w.code = (code & ~15) | bo.long_R | kLongBit;
+        w.read2 = -1;
+        w.out2_begin = 0;
+        items.push_back(w);
+        cost.push_back(rows * (std::max(m, m2) + 1 + kWarp) * (two ? 2 : 1));
+        sl.cells += (int64_t)n * (m + m2);
+        sl.pairs += two ? 2 : 1;
+        h += two ? 2 : 1;
+      }
+    };
     // emit the haplotype runs of read r (and r2 >= 0 riding along)
     auto emit = [&](int64_t r, int64_t r2) {
       const int32_t code = c.read_code[r - c.ra];
@@ -619,6 +653,10 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       const int32_t code = c.read_code[r - c.ra];
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
       if (n <= 0) continue;
+      if (bo.long_warp && fp32 && !anchored && !code_general(code) && (code & 512) != 0) {
+        emit_long(r);
+        continue;
+      }
       const bool eligible = pair_reads && !anchored && !code_general(code) && (code & 512) == 0 &&
                             ((bo.pair_mask >> code_R(code)) & 1);
       if (!eligible) { emit(r, -1); continue; }
@@ -655,6 +693,8 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   c.n_paired = (int64_t)(mid - c.items.begin());
   auto wide = std::stable_partition(c.items.begin(), mid, [](const WorkItem& w) { return code_R(w.code) >= 6; });
   c.n_paired_wide = (int64_t)(wide - c.items.begin());
+  auto lend = std::stable_partition(mid, c.items.end(), [](const WorkItem& w) { return code_long(w.code); });
+  c.n_long = (int64_t)(lend - mid);
 }
 
 // Pair form: pairs grouped by read (counting sort), each read's haplotypes as
@@ -760,7 +800,8 @@ Layout layout_for(const HostChunk& c, const vd_batch* b, int64_t warps) {
   L.o_sp1 = take((size_t)std::max<int64_t>(1, c.pairs_scored) * sizeof(RescueEntry));
   L.o_sp2 = take((size_t)std::max<int64_t>(1, c.pairs_scored) * sizeof(RescueEntry));
   L.o_cnt = take(16 * sizeof(unsigned long long));
-  L.scratch_stride = c.any_long ? (int64_t)c.max_hap + 1 : 0;
+  // the long-read kernel keeps two boundary buffers per warp slot
+  L.scratch_stride = c.any_long ? (int64_t)(c.max_hap + 1) * (c.n_long > 0 ? 2 : 1) : 0;
   L.warps = c.any_strip ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
   L.o_scratch = take((size_t)std::max<int64_t>(1, L.scratch_stride) * warps * sizeof(double2));
   L.total = off;
@@ -902,7 +943,8 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   cudaGetLastError();  // launch checks below must see only their own errors
   // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag,
   // cnt[6..7] heads of the two-read kernels, cnt[8] spill count of the FP64
-  // tier and cnt[9] head of the drift tier (FP32 semiglobal only)
+  // tier, cnt[9] head of the drift tier (FP32 semiglobal only) and cnt[10]
+  // head of the long-read kernel
   VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), pl->stream));
   VD_CUDA(cudaEventRecordWithFlags(pl->ev_begin, pl->stream, evflags));
   const BatchView bv = batch_view(pl);
@@ -940,9 +982,21 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       if (err != cudaSuccess) return cuda_fail(err, "two-read tier launch");
       ++n;
     }
-    q.items = (const WorkItem*)(d + L.o_items) + np;
-    q.n_items = (long long)(pl->chunk.items.size() - np);
     q.static_order = pl->params.schedule == VD_SCHEDULE_PLAIN ? 1 : 0;
+    const int64_t nl = pl->chunk.n_long;
+    if (nl > 0) {
+      // long reads, two haplotypes per warp; their failures join the spill list
+      QueueView ql = q;
+      ql.items = (const WorkItem*)(d + L.o_items) + np;
+      ql.n_items = nl;
+      ql.head = cnt + 10;
+      const int R = pl->chunk.long_R;
+      err = launch_long_f32(R, bv, ql, &dt->f32, ht->s32d, e->grid_long[R == 8 ? 1 : 0], pl->stream);
+      if (err != cudaSuccess) return cuda_fail(err, "long-read tier launch");
+      ++n;
+    }
+    q.items = (const WorkItem*)(d + L.o_items) + np + nl;
+    q.n_items = (long long)(pl->chunk.items.size() - np - nl);
     if (q.n_items > 0) {
       err = f64 ? launch_f64(anch, bv, q, &dt->f64, ht->s64, 1, e->grid[1][anch], pl->stream)
                 : launch_f32(anch, bv, q, &dt->f32, ht->s32, 0, e->grid[0][anch], pl->stream);
@@ -1065,6 +1119,12 @@ int init_engine_grids(vd_engine* e) {
   if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
   // its warps index the strip scratch, which is sized by the largest grid
   e->grid_drift = std::min(std::max(1, bps) * e->sm_count, e->grid[0][0]);
+  for (int k = 0; k < 2; ++k) {
+    bps = 0;
+    err = occupancy_long_f32(k ? 8 : 4, &bps);
+    if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+    e->grid_long[k] = std::min(std::max(1, bps) * e->sm_count, e->grid[0][0]);
+  }
   for (int f = 0; f < 2; ++f) {
     bps = 0;
     err = occupancy_grad(f != 0, &bps);
@@ -1230,7 +1290,9 @@ int vd_engine_set_tuning(vd_engine* e, const vd_tuning* t) {
   if (t->pair_mask & ~0x1fe) return fail(VD_EINVAL, "pair_mask holds bits 1..8 only");
   if (t->max_item_columns < 0) return fail(VD_EINVAL, "max_item_columns must be >= 0");
   if (t->pipeline_gcells < 0) return fail(VD_EINVAL, "pipeline_gcells must be >= 0");
-  for (int i = 0; i < 4; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  if (t->long_mode != VD_LONG_WARP && t->long_mode != VD_LONG_SINGLE)
+    return fail(VD_EINVAL, "long_mode must be VD_LONG_WARP or VD_LONG_SINGLE");
+  for (int i = 0; i < 3; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
   std::lock_guard<std::mutex> lk(e->mu);
   e->tuning = *t;
   return VD_OK;
@@ -1318,7 +1380,8 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   for (int64_t h = 0; h < b->n_haps; ++h) max_hap = std::max<int64_t>(max_hap, b->hap_off[h + 1] - b->hap_off[h]);
   for (int64_t r = 0; r < b->n_reads; ++r) max_read = std::max<int64_t>(max_read, b->read_off[r + 1] - b->read_off[r]);
   const int64_t scratch_warps = max_read + p->anchored > kStripRows ? warps : std::min<int64_t>(warps, (int64_t)kRobustBlocks * kWarpsPerBlock);
-  fixed += (max_hap + 1) * scratch_warps * (int64_t)sizeof(double2) + 64 * 1024;
+  // (two boundary buffers per warp slot when the long-read kernel runs)
+  fixed += (max_hap + 1) * scratch_warps * (int64_t)sizeof(double2) * (max_read > kStripRows ? 2 : 1) + 64 * 1024;
   const int64_t budget = (int64_t)e->budget;
 
   // results of the chunk in a slot, once its stream has completed

@@ -517,11 +517,18 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
 // serves both reads (fma.rn.f32x2): per two cells 2 compares, 2 predicated
 // multiplies and 4 packed FMAs instead of 12 scalar instructions, and the
 // haplotype base load, the ramp and the per-step bookkeeping are shared.
+//
+// Per row the lane keeps W = x*om + mu of the column it finished -- the
+// deletion state om of the NEXT column, computed as soon as mu is known --
+// and s; mu itself is not kept.  The next column reads om from W, so the
+// arithmetic (and every bit of the result) is that of column(): the same FMA
+// on the same operands, one column earlier, and a row holds 2 state words
+// instead of 3.
 template <int R>
 struct PairRows {
   uint32_t ra[R], rb[R];       // read bases of the two reads
   float2 miss[R], K[R], X[R];  // per-row factors (x: first read, y: second)
-  float2 mu[R], om[R], s[R];   // state of the previous column
+  float2 W[R], s[R];           // om of the next column, and s, of the column finished last
 };
 
 template <int R>
@@ -534,12 +541,11 @@ __device__ __forceinline__ void column2(PairRows<R>& w, uint32_t hb, float2 s_to
     float2 mu_new = s_above;
     mul_if_ne(mu_new.x, w.ra[r], hb, w.miss[r].x);
     mul_if_ne(mu_new.y, w.rb[r], hb, w.miss[r].y);
-    const float2 om_new = __ffma2_rn(x, w.om[r], w.mu[r]);
+    const float2 om_new = w.W[r];
     const float2 u_new = __ffma2_rn(w.X[r], nu, mu_new);
     const float2 s_new = __ffma2_rn(k2, om_new, __ffma2_rn(w.K[r], nu, mu_new));
     s_above = w.s[r];
-    w.mu[r] = mu_new;
-    w.om[r] = om_new;
+    w.W[r] = __ffma2_rn(x, om_new, mu_new);
     w.s[r] = s_new;
     nu = u_new;
   }
@@ -627,8 +633,7 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
       rw.K[r].y = 0.f;
       rw.X[r].y = 1.f;
     }
-    rw.mu[r] = make_float2(0.f, 0.f);
-    rw.om[r] = make_float2(0.f, 0.f);
+    rw.W[r] = make_float2(0.f, 0.f);
     rw.s[r] = make_float2(0.f, 0.f);
   }
 
@@ -659,10 +664,9 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   double accA = 0.0, accB = 0.0;
   // snapshot layout, 16-byte entries slot-major with one entry per lane (the
   // lane that saves or restores is alone in its branch, so its instruction
-  // count is what costs): (mu, om) of each row, s of two rows, (s_top, FP32
-  // row sums), the two FP64 row sums
-  constexpr int kSPairs = (R + 1) / 2;
-  double2* const svd = reinterpret_cast<double2*>(sv + (R + kSPairs + 1) * kWarp);
+  // count is what costs): (W, s) of each row, (s_top, FP32 row sums), the two
+  // FP64 row sums
+  double2* const svd = reinterpret_cast<double2*>(sv + (R + 1) * kWarp);
 
   // the warp writes haplotype k's ring entry (every lane computes it, lane 0
   // stores it)
@@ -707,30 +711,18 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
   };
   auto save = [&]() {
 #pragma unroll
-    for (int r = 0; r < R; ++r)
-      sv[r * kWarp + lane] = make_float4(rw.mu[r].x, rw.mu[r].y, rw.om[r].x, rw.om[r].y);
-#pragma unroll
-    for (int r = 0; r < R; r += 2) {
-      const float2 b = (r + 1 < R) ? rw.s[r + 1] : make_float2(0.f, 0.f);
-      sv[(R + r / 2) * kWarp + lane] = make_float4(rw.s[r].x, rw.s[r].y, b.x, b.y);
-    }
-    sv[(R + kSPairs) * kWarp + lane] = make_float4(s_top.x, s_top.y, acc32.x, acc32.y);
+    for (int r = 0; r < R; ++r) sv[r * kWarp + lane] = make_float4(rw.W[r].x, rw.W[r].y, rw.s[r].x, rw.s[r].y);
+    sv[R * kWarp + lane] = make_float4(s_top.x, s_top.y, acc32.x, acc32.y);
     svd[lane] = make_double2(accA, accB);
   };
   auto restore = [&]() {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const float4 v = sv[r * kWarp + lane];
-      rw.mu[r] = make_float2(v.x, v.y);
-      rw.om[r] = make_float2(v.z, v.w);
+      rw.W[r] = make_float2(v.x, v.y);
+      rw.s[r] = make_float2(v.z, v.w);
     }
-#pragma unroll
-    for (int r = 0; r < R; r += 2) {
-      const float4 v = sv[(R + r / 2) * kWarp + lane];
-      rw.s[r] = make_float2(v.x, v.y);
-      if (r + 1 < R) rw.s[r + 1] = make_float2(v.z, v.w);
-    }
-    const float4 v = sv[(R + kSPairs) * kWarp + lane];
+    const float4 v = sv[R * kWarp + lane];
     s_top = make_float2(v.x, v.y);
     acc32 = make_float2(v.z, v.w);
     const double2 a = svd[lane];
@@ -757,8 +749,7 @@ __device__ __noinline__ void process_pair(const BatchView bv, const QueueView qv
         } else {
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            rw.mu[r] = make_float2(0.f, 0.f);
-            rw.om[r] = make_float2(0.f, 0.f);
+            rw.W[r] = make_float2(0.f, 0.f);
             rw.s[r] = make_float2(0.f, 0.f);
           }
           s_top = make_float2(0.f, 0.f);
@@ -938,17 +929,20 @@ pairhmm_kernel(const BatchView bv, const QueueView qv, const Tables<T>* __restri
 
 // Persistent kernels of the two-read items (FP32, semiglobal), on their own
 // work list ahead of the single-read items of the same tier.  Packed rows
-// need about 14 registers each: items with 6-8 rows per lane run 3 blocks per
+// need about 12 registers each: items with 6-8 rows per lane run 3 blocks per
 // SM (168 registers), items with up to 5 rows 4 blocks (128 registers), each
-// kernel instantiating only its own row counts.
-template <int kLoR, int kHiR, int kBlocks>
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
+// kernel instantiating only its own row counts.  (Resident warps come in
+// steps of 4 per SM whatever the block size: each of the 4 schedulers holds
+// a quarter of the register file, so 13-15 warps need no more than 128
+// registers either.)
+template <int kLoR, int kHiR, int kBlocks, int kWarps = kWarpsPerBlock>
+__global__ void __launch_bounds__(kWarps * kWarp, kBlocks)
 pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
                     const Scalars<float> sc) {
   __shared__ Tables<float> tab;
   // per warp: the lane states laid down at a shared haplotype prefix
-  __shared__ float4 saves[kWarpsPerBlock][(kHiR + (kHiR + 1) / 2 + 2) * kWarp];
-  __shared__ HapMeta meta[kWarpsPerBlock][kMetaRing];
+  __shared__ float4 saves[kWarps][(kHiR + 2) * kWarp];
+  __shared__ HapMeta meta[kWarps][kMetaRing];
   {
     const int words = (int)(sizeof(Tables<float>) / sizeof(int));
     const int* src = reinterpret_cast<const int*>(gtab);

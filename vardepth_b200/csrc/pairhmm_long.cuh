@@ -1,0 +1,348 @@
+// Long reads (more rows than one 256-row strip), FP32, semiglobal: one warp
+// runs one read against TWO haplotypes of its region at once.
+//
+// The read's rows are packed as float2 over the two haplotypes (x: the first,
+// y: the second), so every FMA serves both pairs (fma.rn.f32x2) and the read's
+// per-row constants, its strip count and its strip bookkeeping are shared: the
+// pairs of one warp always have the same number of strips, which two reads of
+// different lengths would not.  A region's haplotypes differ by a few small
+// edits, so their lengths nearly agree and the shorter one idles for a few
+// columns at most.
+//
+// Range.  An error-rich read (8% errors at reported Q30) loses about one bit
+// per row along its best path, far more over a 256-row strip than FP32 holds,
+// so each strip is given B boost bits: lane L multiplies the two values it
+// receives from the lane above (or the strip boundary) by 2^k_L, k_L being
+// lane L's share of B.  A boost on a lane's inputs scales the lane's rows and
+// everything below by an exact power of two, so the rows keep the one-sided
+// emission (a match costs no multiply) and the boosts are undone exactly in
+// the final exponent.  B is measured as the read goes: strip s+1 takes the
+// decay strip s showed at its bottom (the exponent of its boundary maximum),
+// and a strip whose bottom leaves 2^-100 .. 2^100 is run again with B
+// corrected by what it measured (its input boundary is kept: the warp's slot
+// holds two boundary buffers, one read and one written).  The first strip
+// has nothing to learn from, so its input starts at 2^100: one pass measures
+// any decay up to about 200 bits.  Strips are renormalised to 2^0 exactly at
+// their end, as the primary tier does.  A pair still out of range after
+// kLongTries runs of a strip goes to the drift and FP64 tiers.
+//
+// Every choice above depends on the pair's own data only (B, the re-runs of a
+// strip and its renormalisation are per half; a re-run caused by the other
+// half recomputes this half's strip bit for bit), so a pair's result is the
+// same whichever haplotype shares its warp, or none; the plain schedule runs
+// one pair per item on this kernel and gives the same bits.
+#pragma once
+#include "pairhmm_kernel.cuh"
+
+namespace vd {
+
+constexpr int kLongTries = 6;       // runs of one strip before a half gives up
+constexpr int kLongWindow = 100;    // a strip bottom must end in 2^-100 .. 2^100
+constexpr int kLongStart = 100;     // the first strip's input, 2^100 (binary orders)
+
+template <int R>
+struct LongRows {
+  uint32_t rb[R];     // read bases (kNeverBase for rows past the read)
+  float miss[R];      // mismatch factor of the row (the same for both halves)
+  float2 K[R], X[R];  // k1 f_i and (x/4) f_i (alpha f_n on the last row), both halves
+  float2 W[R], s[R];  // om of the next column and s of the column finished last
+};
+
+template <int R>
+__device__ __forceinline__ void column_long(LongRows<R>& w, uint32_t hbx, uint32_t hby, float2 s_top, float2 u_top,
+                                            float2 k2, float2 x, float2& u_bot) {
+  float2 s_above = s_top;
+  float2 nu = u_top;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    float2 mu_new = s_above;
+    mul_if_ne(mu_new.x, w.rb[r], hbx, w.miss[r]);
+    mul_if_ne(mu_new.y, w.rb[r], hby, w.miss[r]);
+    const float2 om_new = w.W[r];
+    const float2 u_new = __ffma2_rn(w.X[r], nu, mu_new);
+    const float2 s_new = __ffma2_rn(k2, om_new, __ffma2_rn(w.K[r], nu, mu_new));
+    s_above = w.s[r];
+    w.W[r] = __ffma2_rn(x, om_new, mu_new);
+    w.s[r] = s_new;
+    nu = u_new;
+  }
+  u_bot = nu;
+}
+
+// exponent of a boundary maximum or final sum, +-1024 for inf/NaN and zero
+__device__ __forceinline__ int long_exponent(float v) {
+  return (v != v || v >= HUGE_VALF) ? 1024 : (v > 0.f ? ilogbf(v) : -1024);
+}
+__device__ __forceinline__ int long_exponent(double v) {
+  return (v != v || v >= HUGE_VAL) ? 1024 : (v > 0.0 ? ilogb(v) : -1024);
+}
+
+// One work item: read w.read against haplotypes hap_begin and hap_begin + 1
+// (nhap = 2) or hap_begin alone (nhap = 1); outputs out_begin (+1).
+// `scratch` is the warp's slot: 2 * half float4 boundary records (half >= the
+// longest haplotype + 1); `ring` 32 float4 of shared memory per warp.
+template <int R>
+__device__ __noinline__ void process_long(const BatchView bv, const QueueView qv, const WorkItem w,
+                                          const Tables<float>* __restrict__ tb, const Scalars<float> sc,
+                                          const int lane, float4* __restrict__ scratch, float4* __restrict__ ring) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr double kLn2 = 0.6931471805599453094;
+  constexpr int SR = kWarp * R;
+  const int64_t roff = bv.read_off[w.read];
+  const int n = (int)(bv.read_off[w.read + 1] - roff);
+  const uint8_t* __restrict__ rbase = bv.read_bases + roff;
+  const uint8_t* __restrict__ rqual = bv.read_quals + roff;
+  const bool two = w.nhap > 1;
+  const int64_t h1 = w.hap_begin, h2 = two ? w.hap_begin + 1 : w.hap_begin;
+  const int64_t ho1 = bv.hap_off[h1], ho2 = bv.hap_off[h2];
+  const int m1 = (int)(bv.hap_off[h1 + 1] - ho1), m2 = (int)(bv.hap_off[h2 + 1] - ho2);
+  const uint8_t* __restrict__ hp1 = bv.hap_bases + ho1 - 1;  // hp[j] = base of column j >= 1
+  const uint8_t* __restrict__ hp2 = bv.hap_bases + ho2 - 1;
+  const int M = max(m1, m2);
+  const int nstrips = (n + SR - 1) / SR;
+  const long long half = qv.scratch_stride / 2;
+
+  double lnN = 0.0;
+  for (int i = lane; i < n; i += kWarp) lnN += tb->lnN[rqual[i]];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) lnN += __shfl_xor_sync(FULL, lnN, o);
+  const float A = tb->A[rqual[n - 1]];
+  const float2 k2 = make_float2(sc.k2, sc.k2), x = make_float2(sc.x, sc.x);
+  const float c0 = sc.c;
+
+  // per half: boost bits of the current strip, total exponent, still in play
+  int Bx = 0, By = 0, Ex = 0, Ey = 0;
+  bool okx = true, oky = two;
+  int lgx = 0, lgy = 0;        // bottom exponents of the last run
+  double zx = 0.0, zy = 0.0;   // final sums (last strip, lane 31)
+
+  // One run of strip `strip` with Bx / By boost bits; reads boundary buffer
+  // src_half, writes the other.  Sets lgx / lgy (bottom maximum or final sum).
+  auto run_strip = [&](const int strip, const bool last) {
+    const int i0 = strip * SR;
+    const int ns = min(SR, n - i0);           // read rows of the strip
+    const int lanes_used = (ns + R - 1) / R;  // lanes holding read rows
+    LongRows<R> rw;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = i0 + lane * R + r;
+      if (i < n) {
+        const unsigned q = rqual[i];
+        rw.rb[r] = rbase[i];
+        rw.miss[r] = tb->miss[q];
+        const float K = tb->K[q], X = (i == n - 1) ? A : tb->X[q];
+        rw.K[r] = make_float2(K, K);
+        rw.X[r] = make_float2(X, X);
+      } else {  // past the read: pass u down the column
+        rw.rb[r] = kNeverBase;
+        rw.miss[r] = 0.f;
+        rw.K[r] = make_float2(0.f, 0.f);
+        rw.X[r] = make_float2(1.f, 1.f);
+      }
+      rw.W[r] = make_float2(0.f, 0.f);
+      rw.s[r] = make_float2(0.f, 0.f);
+    }
+    // lane L's share of the boost: floor((L+1) B / lanes) - floor(L B / lanes)
+    // over the lanes holding read rows; the first strip's input starts at 2^kLongStart
+    // (|B| <= 4 ns keeps every share within +-4R, far inside the float exponent range)
+    int kx = 0, ky = 0;
+    if (lane < lanes_used) {
+      kx = (lane + 1) * Bx / lanes_used - lane * Bx / lanes_used;
+      ky = (lane + 1) * By / lanes_used - lane * By / lanes_used;
+    }
+    const float2 bf = make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f));
+    const float cin = c0 * pow2T(kLongStart, 0.f);  // the first strip's row-0 value
+    float4* const src = scratch + (long long)(strip & 1) * half;
+    float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
+
+    float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
+    double accx = 0.0, accy = 0.0;
+    float bmx = 0.f, bmy = 0.f;
+    // boundary records of the strip above, staged through the warp's ring:
+    // every 32 steps each lane loads one record of the next 32 columns
+    float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto load_window = [&](int base) -> float4 {
+      const int p = base + lane;
+      return (strip > 0 && p <= M) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    nxt = load_window(0);
+    const int steps = M + 1 + (kWarp - 1);
+    for (int t = 0; t < steps; ++t) {
+      if ((t & (kWarp - 1)) == 0) {
+        __syncwarp();
+        ring[lane] = nxt;
+        __syncwarp();
+        nxt = load_window(t + kWarp);
+      }
+      const int p = t - lane;  // this lane's column
+      float2 u_in = shfl_up2(u_bot);
+      float2 s_in = shfl_up2(rw.s[R - 1]);
+      if (lane == 0) {
+        if (strip == 0) {
+          u_in = make_float2(cin, cin);
+          s_in = u_in;
+        } else {
+          const float4 rec = ring[t & (kWarp - 1)];
+          s_in = make_float2(rec.x, rec.z);
+          u_in = make_float2(rec.y, rec.w);
+        }
+      }
+      u_in = __fmul2_rn(u_in, bf);
+      s_in = __fmul2_rn(s_in, bf);
+      const bool inside = p >= 0 && p <= M;
+      // column 0 has no base (kNeverBase never matches); past a haplotype's
+      // end its half reads that haplotype's last base (its columns are not used)
+      const uint32_t hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
+      const uint32_t hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
+      column_long<R>(rw, hbx, hby, p > 0 ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
+      if (p <= 0) {
+        // column 0 (and the lanes not started yet): no diagonal, no deletions
+#pragma unroll
+        for (int r = 0; r < R; ++r) rw.W[r] = make_float2(0.f, 0.f);
+      }
+      s_top = s_in;
+      if (lane == kWarp - 1 && inside) {
+        if (last) {
+          // the final row sums, flushed into FP64 after every column 8r+7
+          if (p <= m1) acc32.x += u_bot.x;
+          if (p <= m2) acc32.y += u_bot.y;
+          if ((p & 7) == 7) {
+            accx += (double)acc32.x;
+            accy += (double)acc32.y;
+            acc32 = make_float2(0.f, 0.f);
+          }
+        } else {
+          dst[p] = make_float4(rw.s[R - 1].x, u_bot.x, rw.s[R - 1].y, u_bot.y);
+          if (p <= m1) bmx = fmaxf(bmx, fmaxf(rw.s[R - 1].x, u_bot.x));
+          if (p <= m2) bmy = fmaxf(bmy, fmaxf(rw.s[R - 1].y, u_bot.y));
+        }
+      }
+    }
+    __syncwarp();
+    if (last) {
+      zx = __shfl_sync(FULL, accx + (double)acc32.x, kWarp - 1);
+      zy = __shfl_sync(FULL, accy + (double)acc32.y, kWarp - 1);
+      lgx = long_exponent(zx);
+      lgy = long_exponent(zy);
+    } else {
+      lgx = long_exponent(__shfl_sync(FULL, bmx, kWarp - 1));
+      lgy = long_exponent(__shfl_sync(FULL, bmy, kWarp - 1));
+    }
+  };
+
+  // the strips, each run until both halves' bottoms are in the window
+  bool fail_x = false, fail_y = !two;
+  for (int strip = 0; strip < nstrips && (okx || oky); ++strip) {
+    const bool last = strip == nstrips - 1;
+    const int ns = min(SR, n - strip * SR);
+    for (int attempt = 0;; ++attempt) {
+      run_strip(strip, last);
+      const bool gx = !okx || (lgx >= -kLongWindow && lgx < kLongWindow);
+      const bool gy = !oky || (lgy >= -kLongWindow && lgy < kLongWindow);
+      if (gx && gy) break;
+      if (attempt + 1 == kLongTries) {
+        if (!gx) { okx = false; fail_x = true; }
+        if (!gy) { oky = false; fail_y = true; }
+        break;
+      }
+      // correct the boost of a half that left the window by what it measured
+      // (half a bit per row when it overflowed or underflowed completely)
+      auto correct = [&](int& B, int lg) {
+        const int step = (lg == 1024) ? -ns / 2 : (lg == -1024) ? ns / 2 : -lg;
+        B = max(-4 * ns, min(4 * ns, B + (step != 0 ? step : (lg > 0 ? -1 : 1))));
+      };
+      if (!gx) correct(Bx, lgx);
+      if (!gy) correct(By, lgy);
+    }
+    // the boosts of the strip count into the exponent (plus the first strip's start)
+    const int start = strip == 0 ? kLongStart : 0;
+    if (!last) {
+      // renormalise the boundary the next strip reads to 2^0 (two exact factors
+      // each, so any shift stays representable); the next strip's boost is this
+      // strip's decay, scaled to its rows
+      float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
+      const int ksx = okx ? -lgx : 0, ksy = oky ? -lgy : 0;
+      const float fx1 = pow2T(ksx / 2, 0.f), fx2 = pow2T(ksx - ksx / 2, 0.f);
+      const float fy1 = pow2T(ksy / 2, 0.f), fy2 = pow2T(ksy - ksy / 2, 0.f);
+      for (int p = lane; p <= M; p += kWarp) {
+        float4 v = dst[p];
+        v.x = (v.x * fx1) * fx2;
+        v.y = (v.y * fx1) * fx2;
+        v.z = (v.z * fy1) * fy2;
+        v.w = (v.w * fy1) * fy2;
+        dst[p] = v;
+      }
+      __syncwarp();
+      const int ns1 = min(SR, n - (strip + 1) * SR);
+      if (okx) {
+        Ex += Bx + start + ksx;
+        Bx = max(0, min(4 * ns1, (Bx + start - lgx) * ns1 / ns));
+      }
+      if (oky) {
+        Ey += By + start + ksy;
+        By = max(0, min(4 * ns1, (By + start - lgy) * ns1 / ns));
+      }
+    } else {
+      Ex += Bx + start;
+      Ey += By + start;
+    }
+  }
+
+  if (lane == kWarp - 1) {
+    const double lnC1 = sc.ln_c + log((double)(m1 + 1));
+    const double lnC2 = sc.ln_c + log((double)(m2 + 1));
+    if (okx && !fail_x) {
+      bv.out[w.out_begin] = log(zx) - lnC1 + lnN - (double)Ex * kLn2;
+    } else {
+      bv.out[w.out_begin] = __longlong_as_double(0x7ff8000000000000LL);
+      spill_pair<float>(qv, w.read, h1, w.out_begin);
+    }
+    if (two) {
+      if (oky && !fail_y) {
+        bv.out[w.out_begin + 1] = log(zy) - lnC2 + lnN - (double)Ey * kLn2;
+      } else {
+        bv.out[w.out_begin + 1] = __longlong_as_double(0x7ff8000000000000LL);
+        spill_pair<float>(qv, w.read, h2, w.out_begin + 1);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Persistent kernel of the long-read items (FP32 semiglobal primary tier):
+// every warp pulls items from qv.head (or walks them in the fixed round-robin
+// order of the plain schedule).  Items whose read has another rows-per-lane
+// count than R are not in its list.
+template <int R, int kBlocks>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
+pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
+                    const Scalars<float> sc) {
+  __shared__ Tables<float> tab;
+  __shared__ float4 rings[kWarpsPerBlock][kWarp];
+  {
+    const int words = (int)(sizeof(Tables<float>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(gtab);
+    int* dst = reinterpret_cast<int*>(&tab);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & (kWarp - 1);
+  const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  float4* scratch = reinterpret_cast<float4*>(qv.scratch) + gw * qv.scratch_stride;
+  const long long stride = (long long)gridDim.x * kWarpsPerBlock;
+  long long next = gw;
+  for (;;) {
+    unsigned long long i = 0;
+    if (qv.static_order) {
+      i = (unsigned long long)next;
+      next += stride;
+    } else {
+      if (lane == 0) i = atomicAdd(qv.head, 1ull);
+      i = __shfl_sync(0xffffffffu, i, 0);
+    }
+    if ((long long)i >= qv.n_items) break;
+    process_long<R>(bv, qv, qv.items[i], &tab, sc, lane, scratch, rings[threadIdx.x >> 5]);
+  }
+}
+
+}  // namespace vd
