@@ -41,7 +41,8 @@ enum {
                                per lane) and ordered longest first; two reads per warp where
                                possible */
   VD_SCHEDULE_PLAIN = 1     /* the comparison baseline: one read x haplotype pair per item, a
-                               fixed tile of 8 rows per lane, items in input order, assigned
+                               fixed tile of 8 rows per lane (reads longer than one strip keep
+                               the engine's strip height), items in input order, assigned
                                round-robin to a fixed grid of warps (no queue, no binning) */
 };
 
@@ -141,11 +142,13 @@ typedef struct vd_tuning {
                            one; 0 = the default (300), 1e6 or more = one chunk */
   int long_mode;        /* reads longer than one strip, FP32 semiglobal: VD_LONG_WARP (default) runs a
                            read against two haplotypes per warp with per-lane power-of-two boosts;
-                           VD_LONG_SINGLE runs them in the single-read kernel (strips renormalised
+                           VD_LONG_BLOCK the same items on a block per item, whose 4 warps split
+                           each strip (4x shorter latency per pair, for batches of few long
+                           pairs); VD_LONG_SINGLE the single-read kernel (strips renormalised
                            exactly, error-rich reads then rescued by the drift tier) */
   int reserved[3];      /* must be zero */
 } vd_tuning;
-enum { VD_LONG_WARP = 0, VD_LONG_SINGLE = 1 };
+enum { VD_LONG_WARP = 0, VD_LONG_SINGLE = 1, VD_LONG_BLOCK = 2 };
 int vd_engine_set_tuning(vd_engine *engine, const vd_tuning *tuning);
 int vd_engine_get_tuning(const vd_engine *engine, vd_tuning *tuning);
 

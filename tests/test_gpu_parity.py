@@ -549,7 +549,9 @@ def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
     """Reads of 257, 1,500 and 10,000 bases in the long-read kernel (one read against two
     haplotypes per warp, per-lane power-of-two boosts): within 1e-4 log10 of the FP64 oracle
     with no pair left to FP64 and the genotype argmax unchanged, bit-identical under the plain
-    schedule (one haplotype per warp) and with 128-row strips within the same bound."""
+    schedule (one haplotype per item).  The same bound and the same plain/batched identity hold
+    for the block-per-pair kernel (the CTA's 4 warps split each 1,024-row strip), for 128-row
+    strips and for the single-read path."""
     w = _long_read_regions(int(err * 1000) + n_haps, [257, 1500, 10000], err, n_haps)
     want = _oracle_workload(w)
     eng = native.Engine(0, 8192)
@@ -560,8 +562,11 @@ def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
     assert st.rescued_fp64 + st.rescued_robust == 0 and st.rescued_fp32 == 0
     assert _argmax_agree(w, got, want) == (w.n_regions, w.n_regions)
     np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], got)
-    eng.set_tuning(long_read_rows=128)
-    assert_mixed_close(eng.forward(_packed(w), batched)[0], want)
-    eng.set_tuning(long_mode=native.VD_LONG_SINGLE)
-    assert_mixed_close(eng.forward(_packed(w), batched)[0], want)
+    # other strip heights and the single-read path: within the bound, plain still bit-identical
+    for rows, mode in [(256, native.VD_LONG_BLOCK), (128, native.VD_LONG_BLOCK), (128, native.VD_LONG_WARP),
+                       (256, native.VD_LONG_SINGLE), (128, native.VD_LONG_SINGLE), (64, native.VD_LONG_WARP)]:
+        eng.set_tuning(long_read_rows=rows, long_mode=mode)
+        other = eng.forward(_packed(w), batched)[0]
+        assert_mixed_close(other, want)
+        np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], other)
     eng.close()

@@ -13,10 +13,13 @@ lays out the work list:
 * ``max_item_columns``  how many haplotype columns one work item streams
   (shorter items balance the tail of the persistent queue, longer ones pay
   the 31-step wavefront ramp less often);
-* ``long_mode``  how reads longer than one strip run: two haplotypes of the
-  read per warp with per-lane power-of-two boosts (``VD_LONG_WARP``), or one
-  pair per warp in the single-read kernel with exact strip renormalisation
-  and the drift tier behind it (``VD_LONG_SINGLE``).
+* ``long_mode``  how reads longer than one strip run: the warp-per-pair or
+  block-per-pair split -- a read against two haplotypes per warp with
+  per-lane power-of-two boosts (``VD_LONG_WARP``), the same items on a whole
+  CTA whose warps split each strip (``VD_LONG_BLOCK``: more parallelism per
+  pair, for batches of few long pairs), or one pair per warp in the
+  single-read kernel with exact strip renormalisation and the drift tier
+  behind it (``VD_LONG_SINGLE``).
 
 ``autotune`` times candidate settings with resident plans (CUDA events around
 the captured tier graph) on a seeded region sample of the caller's batch,
@@ -35,7 +38,7 @@ from . import native
 
 DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0, "long_mode": native.VD_LONG_WARP}
 SPACE = {
-    "long_mode": [native.VD_LONG_WARP, native.VD_LONG_SINGLE],
+    "long_mode": [native.VD_LONG_WARP, native.VD_LONG_BLOCK, native.VD_LONG_SINGLE],
     "long_read_rows": [256, 128, 64],
     "pair_mask": [0x1FE, 0x1F0, 0],
     "max_item_columns": [0, 16384, 4096],

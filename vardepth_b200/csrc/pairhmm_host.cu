@@ -184,7 +184,7 @@ struct vd_engine {
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair[2] = {0, 0};          // blocks of the two-read kernels [wide]
   int grid_drift = 0;                 // blocks of the drift tier (no more than grid[0][0])
-  int grid_long[2] = {0, 0};          // blocks of the long-read kernel [R == 8] (no more than grid[0][0])
+  int grid_long[2][2] = {{0, 0}, {0, 0}};  // blocks of the long-read kernels [block][R == 8] (<= grid[0][0])
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
   vd_tuning tuning{256, 0x1fe, 0, 0, VD_LONG_WARP, {0, 0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
@@ -300,7 +300,8 @@ int64_t batch_outputs(const vd_batch* b) {
 // Work-list choices the engine's tuning sets (vd_tuning).
 struct BuildOpts {
   int long_R = kMaxR;              // rows per lane of reads longer than one 256-row strip
-  bool long_warp = true;           // such reads (FP32 semiglobal) run two haplotypes per warp
+  bool long_warp = true;           // such reads (FP32 semiglobal) run a read against two haplotypes per item
+  bool long_block = false;         // ... on a block per item (the CTA's warps split each strip)
   int pair_mask = 0x1fe;           // bit R: two reads of R rows per lane may share a warp
   int64_t max_stream = 1 << 30;    // haplotype columns one work item streams at most
 };
@@ -317,7 +318,9 @@ BuildOpts build_opts(const vd_engine* e) {
   bo.long_R = e->tuning.long_read_rows / kWarp;
   bo.pair_mask = e->tuning.pair_mask;
   bo.max_stream = e->tuning.max_item_columns > 0 ? (int64_t)e->tuning.max_item_columns : (int64_t)1 << 30;
-  bo.long_warp = e->tuning.long_mode == VD_LONG_WARP && (bo.long_R == 8 || bo.long_R == 4);
+  bo.long_warp = (e->tuning.long_mode == VD_LONG_WARP || e->tuning.long_mode == VD_LONG_BLOCK) &&
+                 (bo.long_R == 8 || bo.long_R == 4);
+  bo.long_block = e->tuning.long_mode == VD_LONG_BLOCK;
   return bo;
 }
 
@@ -348,8 +351,9 @@ struct HostChunk {
   bool any_strip = false;          // a read longer than one 256-row strip (every tier strip-mines it)
   int64_t n_paired = 0;            // leading items that carry two reads (own kernels)
   int64_t n_paired_wide = 0;       // the first of them, with 6-8 rows per lane
-  int64_t n_long = 0;              // the items after them: long reads, two haplotypes per warp
+  int64_t n_long = 0;              // the items after them: long reads, two haplotypes per item
   int long_R = kMaxR;              // rows per lane of those
+  bool long_block = false;         // and their kernel: block per item (else warp per item)
 };
 
 // The robust tier runs on a small grid: it only sees pairs the FP64 wavefront
@@ -528,6 +532,7 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   const bool fp32 = pair_reads;  // mixed precision: the FP32 kernels run the primary tier
   if (plain) pair_reads = false;
   c.long_R = bo.long_R;
+  c.long_block = bo.long_block;
   c.ra = b->region_read_off[g0];
   c.rb = b->region_read_off[g1];
   c.ha = b->region_hap_off[g0];
@@ -604,8 +609,11 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       const int32_t code = c.read_code[r - c.ra];
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
       const int n2 = r2 >= 0 ? (int)(c.read_off[r2 - c.ra + 1] - c.read_off[r2 - c.ra]) : 0;
-      const int R = plain ? kMaxR : code_R(code);
-      const int item_code = plain ? (code & ~15) | kMaxR : code;
+      // the plain schedule's fixed tile is 8 rows per lane; reads longer than a
+      // strip keep the tuned strip height in both schedules (same strips, same bits)
+      const bool fixed_tile = plain && (code & 512) == 0;
+      const int R = fixed_tile ? kMaxR : code_R(code);
+      const int item_code = fixed_tile ? (code & ~15) | kMaxR : code;
       const int n_rows = n + (anchored ? 1 : 0);
       const int64_t rows = (int64_t)kWarp * R * ((n_rows + kWarp * R - 1) / (kWarp * R));
       const bool multistrip = n_rows > kStripRows;
@@ -724,7 +732,9 @@ void build_pair_chunk(const vd_batch* b, const PairGroups& pg, int64_t ra, int64
   std::vector<int64_t> cost;
   const int64_t kMaxStream = bo.max_stream;
   for (int64_t r = ra; r < rb; ++r) {
-    const int32_t code = plain ? (c.read_code[r - ra] & ~15) | kMaxR : c.read_code[r - ra];
+    // the fixed tile of the plain schedule (reads longer than a strip keep the tuned strip height)
+    const int32_t rc = c.read_code[r - ra];
+    const int32_t code = (plain && (rc & 512) == 0) ? (rc & ~15) | kMaxR : rc;
     const int n = (int)(c.read_off[r - ra + 1] - c.read_off[r - ra]);
     const int R = code_R(code);
     const int n_rows = n + (anchored ? 1 : 0);
@@ -991,7 +1001,8 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       ql.n_items = nl;
       ql.head = cnt + 10;
       const int R = pl->chunk.long_R;
-      err = launch_long_f32(R, bv, ql, &dt->f32, ht->s32d, e->grid_long[R == 8 ? 1 : 0], pl->stream);
+      const bool blk = pl->chunk.long_block;
+      err = launch_long_f32(R, blk, bv, ql, &dt->f32, ht->s32d, e->grid_long[blk ? 1 : 0][R == 8 ? 1 : 0], pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "long-read tier launch");
       ++n;
     }
@@ -1119,12 +1130,13 @@ int init_engine_grids(vd_engine* e) {
   if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
   // its warps index the strip scratch, which is sized by the largest grid
   e->grid_drift = std::min(std::max(1, bps) * e->sm_count, e->grid[0][0]);
-  for (int k = 0; k < 2; ++k) {
-    bps = 0;
-    err = occupancy_long_f32(k ? 8 : 4, &bps);
-    if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
-    e->grid_long[k] = std::min(std::max(1, bps) * e->sm_count, e->grid[0][0]);
-  }
+  for (int blk = 0; blk < 2; ++blk)
+    for (int k = 0; k < 2; ++k) {
+      bps = 0;
+      err = occupancy_long_f32(k ? 8 : 4, blk != 0, &bps);
+      if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+      e->grid_long[blk][k] = std::min(std::max(1, bps) * e->sm_count, e->grid[0][0]);
+    }
   for (int f = 0; f < 2; ++f) {
     bps = 0;
     err = occupancy_grad(f != 0, &bps);
@@ -1290,8 +1302,8 @@ int vd_engine_set_tuning(vd_engine* e, const vd_tuning* t) {
   if (t->pair_mask & ~0x1fe) return fail(VD_EINVAL, "pair_mask holds bits 1..8 only");
   if (t->max_item_columns < 0) return fail(VD_EINVAL, "max_item_columns must be >= 0");
   if (t->pipeline_gcells < 0) return fail(VD_EINVAL, "pipeline_gcells must be >= 0");
-  if (t->long_mode != VD_LONG_WARP && t->long_mode != VD_LONG_SINGLE)
-    return fail(VD_EINVAL, "long_mode must be VD_LONG_WARP or VD_LONG_SINGLE");
+  if (t->long_mode != VD_LONG_WARP && t->long_mode != VD_LONG_SINGLE && t->long_mode != VD_LONG_BLOCK)
+    return fail(VD_EINVAL, "long_mode must be VD_LONG_WARP, VD_LONG_SINGLE or VD_LONG_BLOCK");
   for (int i = 0; i < 3; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
   std::lock_guard<std::mutex> lk(e->mu);
   e->tuning = *t;

@@ -18,10 +18,11 @@ cudaError_t occupancy_pair_f32(bool wide, int* blocks_per_sm);
 cudaError_t launch_drift_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                              const Scalars<float>& sc, int grid, cudaStream_t stream);
 cudaError_t occupancy_drift_f32(int* blocks_per_sm);
-// long reads, two haplotypes per warp (pairhmm_long.cuh), R = 8 or 4 rows per lane
-cudaError_t launch_long_f32(int R, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
+// long reads, a read against two haplotypes per item (pairhmm_long.cuh), R = 8 or 4 rows
+// per lane; block: the CTA's warps split each strip (block per item), else warp per item
+cudaError_t launch_long_f32(int R, bool block, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                             const Scalars<float>& sc, int grid, cudaStream_t stream);
-cudaError_t occupancy_long_f32(int R, int* blocks_per_sm);
+cudaError_t occupancy_long_f32(int R, bool block, int* blocks_per_sm);
 // gradient kernel (pairhmm_backward.cuh), FP32 and FP64 passes
 struct GradTables;
 struct GradScalars;

@@ -345,4 +345,348 @@ pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
   }
 }
 
+// ---- block per pair: the warps of a CTA split each strip -----------------------
+//
+// The CTA's kWarpsPerBlock warps run one item together over tall strips of
+// W = kWarpsPerBlock times 32 R rows: warp w owns rows 32 R w .. 32 R (w+1) - 1
+// of each tall strip, so a pair's strips run side by side instead of one after
+// another, which shortens a long pair's latency W-fold when few long pairs
+// fill the GPU.  Warp w's bottom row reaches warp w+1 through a shared-memory
+// ring: warp w runs kLongLag steps behind warp w-1 and the block meets at a
+// barrier every kLongChunk steps, so a column is always written one chunk or
+// more before it is read and overwritten two chunks or more after (lane 31 of
+// warp w-1 produces column c at its step c + 31, lane 0 of warp w reads it at
+// its step c, kLongLag - 31 > kLongChunk steps later; the ring holds
+// kLongRing >= kLongChunk + kLongLag columns).  Every warp takes the same
+// number of chunks and barriers whatever its share of the strip, so the
+// barriers always complete.  Each warp has its own boost rate (the decay of
+// its own rows, measured at its bottom), the tall strip is renormalised
+// exactly at its end, and a tall strip whose warps' bottoms leave the window
+// is run again with each warp's rate corrected by what it measured.
+constexpr int kLongChunk = 32;
+constexpr int kLongLag = 64;
+constexpr int kLongRing = 128;
+static_assert(kLongLag - (kWarp - 1) > kLongChunk, "a column must be written a chunk before it is read");
+static_assert(kLongRing >= kLongChunk + kLongLag, "the ring must hold every column in flight");
+
+struct LongBlockShared {
+  float4 hand[kWarpsPerBlock - 1][kLongRing];  // warp w -> w+1 bottom rows (s.x, u.x, s.y, u.y)
+  float4 ring0[kWarp];                          // warp 0: boundary records of the tall strip above
+  int lg[kWarpsPerBlock][2];                    // bottom exponents of the last run
+  int B[kWarpsPerBlock][2];                     // boost bits of each warp's rows
+  double z[2];                                  // final sums
+  long long item;
+};
+
+template <int R>
+__device__ __noinline__ void process_long_block(const BatchView bv, const QueueView qv, const WorkItem w,
+                                                const Tables<float>* __restrict__ tb, const Scalars<float> sc,
+                                                const int lane, const int wid, float4* __restrict__ scratch,
+                                                LongBlockShared& sh) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr double kLn2 = 0.6931471805599453094;
+  constexpr int SR = kWarp * R;
+  constexpr int NW = kWarpsPerBlock;
+  constexpr int H = NW * SR;
+  const int tid = wid * kWarp + lane;
+  const int64_t roff = bv.read_off[w.read];
+  const int n = (int)(bv.read_off[w.read + 1] - roff);
+  const uint8_t* __restrict__ rbase = bv.read_bases + roff;
+  const uint8_t* __restrict__ rqual = bv.read_quals + roff;
+  const bool two = w.nhap > 1;
+  const int64_t h1 = w.hap_begin, h2 = two ? w.hap_begin + 1 : w.hap_begin;
+  const int64_t ho1 = bv.hap_off[h1], ho2 = bv.hap_off[h2];
+  const int m1 = (int)(bv.hap_off[h1 + 1] - ho1), m2 = (int)(bv.hap_off[h2 + 1] - ho2);
+  const uint8_t* __restrict__ hp1 = bv.hap_bases + ho1 - 1;
+  const uint8_t* __restrict__ hp2 = bv.hap_bases + ho2 - 1;
+  const int M = max(m1, m2);
+  const int ntall = (n + H - 1) / H;
+  const long long half = qv.scratch_stride / 2;
+  const int steps = M + 1 + (kWarp - 1);
+  const int chunks = (steps + (NW - 1) * kLongLag + kLongChunk - 1) / kLongChunk;
+
+  double lnN = 0.0;
+  for (int i = lane; i < n; i += kWarp) lnN += tb->lnN[rqual[i]];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) lnN += __shfl_xor_sync(FULL, lnN, o);
+  const float A = tb->A[rqual[n - 1]];
+  const float2 k2 = make_float2(sc.k2, sc.k2), x = make_float2(sc.x, sc.x);
+  const float cin = sc.c * pow2T(kLongStart, 0.f);
+
+  if (tid < NW * 2) sh.B[tid >> 1][tid & 1] = 0;
+  __syncthreads();
+  // per half, identical in every thread: total exponent, still in play
+  int Ex = 0, Ey = 0;
+  bool okx = true, oky = two;
+
+  // one run of tall strip S; the warps' bottom exponents (or the final sums) land in sh
+  auto run_tall = [&](const int S, const int active, const bool last) {
+    const int i0 = S * H + wid * SR;                 // first row of this warp
+    const int ns = min(SR, n - i0);                  // its read rows (<= 0: idle)
+    const int lanes_used = ns > 0 ? (ns + R - 1) / R : 0;
+    const int Bx = sh.B[wid][0], By = sh.B[wid][1];
+    LongRows<R> rw;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = i0 + lane * R + r;
+      if (i < n) {
+        const unsigned q = rqual[i];
+        rw.rb[r] = rbase[i];
+        rw.miss[r] = tb->miss[q];
+        const float K = tb->K[q], X = (i == n - 1) ? A : tb->X[q];
+        rw.K[r] = make_float2(K, K);
+        rw.X[r] = make_float2(X, X);
+      } else {
+        rw.rb[r] = kNeverBase;
+        rw.miss[r] = 0.f;
+        rw.K[r] = make_float2(0.f, 0.f);
+        rw.X[r] = make_float2(1.f, 1.f);
+      }
+      rw.W[r] = make_float2(0.f, 0.f);
+      rw.s[r] = make_float2(0.f, 0.f);
+    }
+    int kx = 0, ky = 0;
+    if (lane < lanes_used) {
+      kx = (lane + 1) * Bx / lanes_used - lane * Bx / lanes_used;
+      ky = (lane + 1) * By / lanes_used - lane * By / lanes_used;
+    }
+    const float2 bf = make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f));
+    float4* const src = scratch + (long long)(S & 1) * half;
+    float4* const dst = scratch + (long long)((S + 1) & 1) * half;
+    const bool bottom = wid == active - 1;  // this warp's bottom row is the tall strip's
+    float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
+    double accx = 0.0, accy = 0.0;
+    float bmx = 0.f, bmy = 0.f;
+    float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto load_window = [&](int base) -> float4 {
+      const int p = base + lane;
+      return (S > 0 && p <= M) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    if (wid == 0) nxt = load_window(0);
+    for (int k = 0; k < chunks; ++k) {
+      for (int uu = 0; uu < kLongChunk; ++uu) {
+        const int t = k * kLongChunk + uu - wid * kLongLag;  // this warp's step (warp-uniform)
+        if (wid >= active || t < 0 || t >= steps) continue;
+        if (wid == 0 && (t & (kWarp - 1)) == 0) {
+          __syncwarp();
+          sh.ring0[lane] = nxt;
+          __syncwarp();
+          nxt = load_window(t + kWarp);
+        }
+        const int p = t - lane;
+        float2 u_in = shfl_up2(u_bot);
+        float2 s_in = shfl_up2(rw.s[R - 1]);
+        if (lane == 0) {
+          if (wid > 0) {
+            const float4 rec = sh.hand[wid - 1][t & (kLongRing - 1)];
+            s_in = make_float2(rec.x, rec.z);
+            u_in = make_float2(rec.y, rec.w);
+          } else if (S == 0) {
+            u_in = make_float2(cin, cin);
+            s_in = u_in;
+          } else {
+            const float4 rec = sh.ring0[t & (kWarp - 1)];
+            s_in = make_float2(rec.x, rec.z);
+            u_in = make_float2(rec.y, rec.w);
+          }
+        }
+        u_in = __fmul2_rn(u_in, bf);
+        s_in = __fmul2_rn(s_in, bf);
+        const bool inside = p >= 0 && p <= M;
+        const uint32_t hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
+        const uint32_t hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
+        column_long<R>(rw, hbx, hby, p > 0 ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
+        if (p <= 0) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) rw.W[r] = make_float2(0.f, 0.f);
+        }
+        s_top = s_in;
+        if (lane == kWarp - 1 && inside) {
+          const float4 rec = make_float4(rw.s[R - 1].x, u_bot.x, rw.s[R - 1].y, u_bot.y);
+          if (bottom && last) {
+            if (p <= m1) acc32.x += u_bot.x;
+            if (p <= m2) acc32.y += u_bot.y;
+            if ((p & 7) == 7) {
+              accx += (double)acc32.x;
+              accy += (double)acc32.y;
+              acc32 = make_float2(0.f, 0.f);
+            }
+          } else {
+            if (bottom) dst[p] = rec;
+            else sh.hand[wid][p & (kLongRing - 1)] = rec;
+            if (p <= m1) bmx = fmaxf(bmx, fmaxf(rec.x, rec.y));
+            if (p <= m2) bmy = fmaxf(bmy, fmaxf(rec.z, rec.w));
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (wid < active) {
+      if (bottom && last) {
+        const double zx = __shfl_sync(FULL, accx + (double)acc32.x, kWarp - 1);
+        const double zy = __shfl_sync(FULL, accy + (double)acc32.y, kWarp - 1);
+        if (lane == 0) {
+          sh.z[0] = zx;
+          sh.z[1] = zy;
+          sh.lg[wid][0] = long_exponent(zx);
+          sh.lg[wid][1] = long_exponent(zy);
+        }
+      } else {
+        const float bx = __shfl_sync(FULL, bmx, kWarp - 1), by = __shfl_sync(FULL, bmy, kWarp - 1);
+        if (lane == 0) {
+          sh.lg[wid][0] = long_exponent(bx);
+          sh.lg[wid][1] = long_exponent(by);
+        }
+      }
+    }
+    __syncthreads();
+  };
+
+  bool fail_x = false, fail_y = !two;
+  for (int S = 0; S < ntall && (okx || oky); ++S) {
+    const int rows = min(H, n - S * H);
+    const int active = (rows + SR - 1) / SR;
+    const bool last = S == ntall - 1;
+    const int start = S == 0 ? kLongStart : 0;
+    auto rows_of = [&](int wi) { return min(SR, rows - wi * SR); };
+    for (int attempt = 0;; ++attempt) {
+      run_tall(S, active, last);
+      // every thread reads the same exponents and takes the same decisions
+      bool gx = !okx, gy = !oky;
+      if (!gx) {
+        gx = true;
+        for (int wi = 0; wi < active; ++wi) gx &= sh.lg[wi][0] >= -kLongWindow && sh.lg[wi][0] < kLongWindow;
+      }
+      if (!gy) {
+        gy = true;
+        for (int wi = 0; wi < active; ++wi) gy &= sh.lg[wi][1] >= -kLongWindow && sh.lg[wi][1] < kLongWindow;
+      }
+      if (gx && gy) break;
+      if (attempt + 1 == kLongTries) {
+        if (!gx) { okx = false; fail_x = true; }
+        if (!gy) { oky = false; fail_y = true; }
+        break;
+      }
+      // each warp's rows get their own measured decay (in: the warp above's
+      // bottom, or the tall strip's input), aiming every bottom at 2^0; a warp
+      // whose bottom over- or underflowed steps by half a bit per row, one fed
+      // by such a warp waits for it
+      __syncthreads();
+      if (tid == 0) {
+        for (int hf = 0; hf < 2; ++hf) {
+          if (hf == 0 ? gx : gy) continue;
+          for (int wi = 0; wi < active; ++wi) {
+            const int in = wi == 0 ? start : sh.lg[wi - 1][hf];
+            const int lg = sh.lg[wi][hf];
+            const int ns = rows_of(wi);
+            int B = sh.B[wi][hf];
+            if (in == 1024 || in == -1024) break;
+            if (lg == 1024 || lg == -1024) {
+              B += lg == 1024 ? -ns / 2 : ns / 2;
+            } else {
+              B = B + in - lg - (wi == 0 ? start : 0);
+            }
+            sh.B[wi][hf] = max(-4 * ns, min(4 * ns, B));
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // exponent bookkeeping, the renormalisation of the boundary and the rates
+    // of the next tall strip (each warp's decay, scaled to its next rows)
+    const int lgb_x = sh.lg[active - 1][0], lgb_y = sh.lg[active - 1][1];
+    int sumBx = 0, sumBy = 0;
+    for (int wi = 0; wi < active; ++wi) { sumBx += sh.B[wi][0]; sumBy += sh.B[wi][1]; }
+    if (!last) {
+      const int ksx = okx ? -lgb_x : 0, ksy = oky ? -lgb_y : 0;
+      float4* const dst = scratch + (long long)((S + 1) & 1) * half;
+      const float fx1 = pow2T(ksx / 2, 0.f), fx2 = pow2T(ksx - ksx / 2, 0.f);
+      const float fy1 = pow2T(ksy / 2, 0.f), fy2 = pow2T(ksy - ksy / 2, 0.f);
+      for (int p = tid; p <= M; p += NW * kWarp) {
+        float4 v = dst[p];
+        v.x = (v.x * fx1) * fx2;
+        v.y = (v.y * fx1) * fx2;
+        v.z = (v.z * fy1) * fy2;
+        v.w = (v.w * fy1) * fy2;
+        dst[p] = v;
+      }
+      if (okx) Ex += sumBx + start + ksx;
+      if (oky) Ey += sumBy + start + ksy;
+      const int rows1 = min(H, n - (S + 1) * H);
+      __syncthreads();
+      if (tid == 0) {
+        for (int hf = 0; hf < 2; ++hf) {
+          for (int wi = 0; wi < NW; ++wi) {
+            const int ns1 = min(SR, rows1 - wi * SR);
+            if (wi >= active || ns1 <= 0) { sh.B[wi][hf] = wi > 0 ? sh.B[wi - 1][hf] : 0; continue; }
+            const int in = wi == 0 ? start : sh.lg[wi - 1][hf];
+            const int d = sh.B[wi][hf] + in - sh.lg[wi][hf];
+            sh.B[wi][hf] = max(0, min(4 * ns1, d * ns1 / rows_of(wi)));
+          }
+        }
+      }
+      __syncthreads();
+    } else {
+      if (okx) Ex += sumBx + start;
+      if (oky) Ey += sumBy + start;
+    }
+  }
+
+  if (tid == 0) {
+    const double lnC1 = sc.ln_c + log((double)(m1 + 1));
+    const double lnC2 = sc.ln_c + log((double)(m2 + 1));
+    if (okx && !fail_x) {
+      bv.out[w.out_begin] = log(sh.z[0]) - lnC1 + lnN - (double)Ex * kLn2;
+    } else {
+      bv.out[w.out_begin] = __longlong_as_double(0x7ff8000000000000LL);
+      spill_pair<float>(qv, w.read, h1, w.out_begin);
+    }
+    if (two) {
+      if (oky && !fail_y) {
+        bv.out[w.out_begin + 1] = log(sh.z[1]) - lnC2 + lnN - (double)Ey * kLn2;
+      } else {
+        bv.out[w.out_begin + 1] = __longlong_as_double(0x7ff8000000000000LL);
+        spill_pair<float>(qv, w.read, h2, w.out_begin + 1);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Persistent block-per-pair kernel of the long-read items: the whole CTA takes
+// one item at a time (thread 0 pulls it, a barrier hands it to the block).
+// Each CTA uses the strip scratch slot of its first warp.
+template <int R, int kBlocks>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
+pairhmm_long_block_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
+                          const Scalars<float> sc) {
+  __shared__ Tables<float> tab;
+  __shared__ LongBlockShared sh;
+  {
+    const int words = (int)(sizeof(Tables<float>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(gtab);
+    int* dst = reinterpret_cast<int*>(&tab);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int wid = threadIdx.x >> 5;
+  float4* scratch = reinterpret_cast<float4*>(qv.scratch) + (long long)blockIdx.x * kWarpsPerBlock * qv.scratch_stride;
+  long long next = blockIdx.x;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (qv.static_order) {
+        sh.item = next;
+        next += gridDim.x;
+      } else {
+        sh.item = (long long)atomicAdd(qv.head, 1ull);
+      }
+    }
+    __syncthreads();
+    const long long i = sh.item;
+    if (i >= qv.n_items) break;
+    process_long_block<R>(bv, qv, qv.items[i], &tab, sc, lane, wid, scratch, sh);
+  }
+}
+
 }  // namespace vd

@@ -20,7 +20,7 @@ VD_OK, VD_EINVAL, VD_ECUDA, VD_ENODEV, VD_ENOMEM, VD_EOVERFLOW = range(6)
 VD_PRECISION_MIXED, VD_PRECISION_FLOAT64 = 0, 1
 VD_SCHEDULE_BATCHED, VD_SCHEDULE_PLAIN = 0, 1
 VD_CHECKPOINT_SQRT, VD_CHECKPOINT_ALL = 0, 1
-VD_LONG_WARP, VD_LONG_SINGLE = 0, 1
+VD_LONG_WARP, VD_LONG_SINGLE, VD_LONG_BLOCK = 0, 1, 2
 
 c_i64 = ctypes.c_int64
 c_i32 = ctypes.c_int32
