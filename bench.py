@@ -481,6 +481,30 @@ def main():
                  "sample_ms_default": best.get("default_ms"), "sample_ms_chosen": best.get("sample_ms"),
                  "trials": tlog, "seconds": round(time.perf_counter() - t0, 2)}
 
+    # ---- the warp-per-pair / block-per-pair split on a batch of few long pairs ----
+    split = None
+    if args.workload == "mixed_length_regions" and world == 1:
+        rl = np.diff(w.read_off)
+        longest = np.maximum.reduceat(rl, w.region_read_off[:-1])
+        long_regions = np.flatnonzero(longest > 256)
+        if len(long_regions):
+            g = int(np.random.default_rng(5).choice(long_regions))
+            one = w.subset([g])
+            op = native.Packed(one.read_bases, one.read_quals, one.read_off, one.hap_bases, one.hap_off,
+                               region_read_off=one.region_read_off, region_hap_off=one.region_hap_off)
+            saved = engine.tuning()
+            split = {"batch": f"one region with {len(one.read_off) - 1} reads of up to {int(longest[g])} bases",
+                     "pairs": one.pairs(), "cells": one.cells(),
+                     "kernel_ms": {}}
+            for name, mode in (("warp", native.VD_LONG_WARP), ("block", native.VD_LONG_BLOCK),
+                               ("single", native.VD_LONG_SINGLE)):
+                engine.set_tuning(**dict(saved, long_mode=mode))
+                p1 = engine.plan(op, params)
+                p1.run()
+                split["kernel_ms"][name] = round(float(np.median([p1.run().kernel_ms for _ in range(3)])), 3)
+                p1.close()
+            engine.set_tuning(**saved)
+
     # ---- device-resident batches (value) ----
     plan = engine.plan(packed, params)
     for _ in range(warm):
@@ -709,7 +733,7 @@ def main():
                          "primary_ms": round(primary_ms, 3),
                          "peak_source": "vd_measure_fp32_peak (FMA loop, this device, this run)",
                          "nominal_peak": round(NOMINAL_FP32_TFLOPS, 1)},
-            "plain": plain, "autotune": tuned, "sharding": sharding,
+            "plain": plain, "autotune": tuned, "long_split_few_pairs": split, "sharding": sharding,
             "cpu_baseline": cpu, "e2e": e2e, "e2e_pairs": e2e_pairs, "gpu_launches": launches,
             "rescued_pairs": int(rescued), "rescued_fraction": round(rescued / max(1, mine.n_outputs()), 6),
             "rescued_fp32_drift_pairs": int(drift_rescued), "parity": parity, "clocks": sampler.summary(),
