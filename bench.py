@@ -312,8 +312,27 @@ def gradient_arm(args, local):
     lo, jo = O.grad_pairs(sw.read_bases, sw.read_quals, sw.read_off, sw.hap_bases, sw.hap_off, pr, ph,
                           O.phred_to_prob(theta0[0]), O.phred_to_prob(theta0[1]), False, theta0[2:])
     tot, want = ref_jac[idx].sum(0), jo.sum(0)
+
+    def per_pair(jac):
+        """Relative error of every pair's Jacobian entries against the oracle (entries of
+        magnitude >= 1e-3; smaller ones by their absolute error), and the pairs above 1e-6."""
+        d = np.abs(jac - jo)
+        rel = d / np.maximum(np.abs(jo), 1e-3)
+        worst = rel.max(axis=1)
+        over = np.flatnonzero(worst > 1e-6)
+        return {"max_rel": float(worst.max()), "p99_rel": float(np.quantile(worst, 0.99)),
+                "median_rel": float(np.median(worst)), "pairs_over_1e-6": int(len(over)),
+                "fraction_over_1e-6": round(len(over) / len(worst), 5),
+                "over_1e-6_read_lengths": sorted({int(sw.read_off[pr[i] + 1] - sw.read_off[pr[i]]) for i in over})[:20]}
+
+    # the same pairs with every pair in the FP64 pass
+    p64, _k64 = AG.params_from_theta(theta0, precision=native.VD_PRECISION_FLOAT64)
+    sub_packed = native.Packed(sw.read_bases, sw.read_quals, sw.read_off, sw.hap_bases, sw.hap_off,
+                               region_read_off=sw.region_read_off, region_hap_off=sw.region_hap_off)
+    _, jac64, _ = engine.forward_backward(sub_packed, p64, native.VD_CHECKPOINT_SQRT)
     check = {"pairs": int(len(idx)), "oracle": "long-double expected-count gradient (oracle/)",
              "summed_gradient_rel_err": [float(v) for v in np.abs(tot - want) / np.abs(want)],
+             "per_pair_mixed": per_pair(ref_jac[idx]), "per_pair_fp64": per_pair(jac64),
              "max_abs_dlog10": float(np.max(np.abs(ref_ln[idx] - lo)) / np.log(10.0))}
     # the fit on every region, from Q45 / Q10 / zero offsets
     batch = AG.Batch(engine, packed)
@@ -635,6 +654,7 @@ def main():
         sample = np.sort(order[:k])
         plist = _pair_list(w, sample)
         scorer = CudaPairHMM(device=local, memory_mb=65536, gap=w.gap, ext=w.ext)
+        scorer.engine.set_tuning(**engine.tuning())  # the autotuned work-list choices, if any
         pl_cells = native.PairList(plist).cells()
         for _ in range(warm):
             res = scorer.score(plist)
