@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
-                    help="run vardepth_b200.autotune on a 2%% region sample first (auto: mixed_length_regions only)")
+                    help="run vardepth_b200.autotune on a 2%% region sample first (auto: every forward workload)")
     ap.add_argument("--workload", default="batched_regions",
                     choices=["batched_regions", "long_haplotype_stress", "planted_error_model", "mixed_length_regions"],
                     help="batched_regions (default) is the metric's workload; the others print their own line")
@@ -487,7 +487,7 @@ def main():
 
     # ---- autotuner: work-list choices timed on a region sample, kept on the engine ----
     tuned = None
-    if args.autotune == "on" or (args.autotune == "auto" and args.workload == "mixed_length_regions"):
+    if args.autotune == "on" or args.autotune == "auto":
         from vardepth_b200 import autotune
         sub = w.subset(autotune.sample_regions(w.region_read_off, w.region_hap_off, fraction=0.02))
         sp = native.Packed(sub.read_bases, sub.read_quals, sub.read_off, sub.hap_bases, sub.hap_off,

@@ -146,7 +146,10 @@ typedef struct vd_tuning {
                            each strip (4x shorter latency per pair, for batches of few long
                            pairs); VD_LONG_SINGLE the single-read kernel (strips renormalised
                            exactly, error-rich reads then rescued by the drift tier) */
-  int reserved[3];      /* must be zero */
+  int pair_split;       /* two-read items with at least this many rows per lane (6, the default, or 7)
+                           run on the 12-warp-per-SM kernel (168 registers), fewer rows on the
+                           16-warp kernel (128 registers); 0 = 6 */
+  int reserved[2];      /* must be zero */
 } vd_tuning;
 enum { VD_LONG_WARP = 0, VD_LONG_SINGLE = 1, VD_LONG_BLOCK = 2 };
 int vd_engine_set_tuning(vd_engine *engine, const vd_tuning *tuning);

@@ -10,6 +10,10 @@ lays out the work list:
   haplotype;
 * ``pair_mask``  which rows-per-lane classes run two reads per warp in the
   packed FP32 kernel (fewer issue slots per cell, more registers per warp);
+* ``pair_split``  the tile of the packed kernels: from how many rows per lane
+  a two-read item runs on the 12-warp-per-SM kernel (168 registers) rather
+  than the 16-warp kernel (128 registers, where 6 rows per lane spill a
+  little);
 * ``max_item_columns``  how many haplotype columns one work item streams
   (shorter items balance the tail of the persistent queue, longer ones pay
   the 31-step wavefront ramp less often);
@@ -36,8 +40,10 @@ import numpy as np
 
 from . import native
 
-DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0, "long_mode": native.VD_LONG_WARP}
+DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0, "long_mode": native.VD_LONG_WARP,
+           "pair_split": 6}
 SPACE = {
+    "pair_split": [6, 7],
     "long_mode": [native.VD_LONG_WARP, native.VD_LONG_BLOCK, native.VD_LONG_SINGLE],
     "long_read_rows": [256, 128, 64],
     "pair_mask": [0x1FE, 0x1F0, 0],

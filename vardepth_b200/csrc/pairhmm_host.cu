@@ -182,11 +182,11 @@ struct vd_engine {
   cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
   std::mutex mu;
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
-  int grid_pair[2] = {0, 0};          // blocks of the two-read kernels [wide]
+  int grid_pair[2][2] = {{0, 0}, {0, 0}};  // blocks of the two-read kernels [split == 7][wide]
   int grid_drift = 0;                 // blocks of the drift tier (no more than grid[0][0])
   int grid_long[2][2] = {{0, 0}, {0, 0}};  // blocks of the long-read kernels [block][R == 8] (<= grid[0][0])
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
-  vd_tuning tuning{256, 0x1fe, 0, 0, VD_LONG_WARP, {0, 0, 0}};  // vd_engine_set_tuning
+  vd_tuning tuning{256, 0x1fe, 0, 0, VD_LONG_WARP, 6, {0, 0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
   DevBuf geno_arena;                  // buffers of vd_region_genotypes
   // table cache
@@ -302,6 +302,7 @@ struct BuildOpts {
   int long_R = kMaxR;              // rows per lane of reads longer than one 256-row strip
   bool long_warp = true;           // such reads (FP32 semiglobal) run a read against two haplotypes per item
   bool long_block = false;         // ... on a block per item (the CTA's warps split each strip)
+  int pair_split = 6;              // two-read items with this many rows per lane or more: 12-warp kernel
   int pair_mask = 0x1fe;           // bit R: two reads of R rows per lane may share a warp
   int64_t max_stream = 1 << 30;    // haplotype columns one work item streams at most
 };
@@ -321,6 +322,7 @@ BuildOpts build_opts(const vd_engine* e) {
   bo.long_warp = (e->tuning.long_mode == VD_LONG_WARP || e->tuning.long_mode == VD_LONG_BLOCK) &&
                  (bo.long_R == 8 || bo.long_R == 4);
   bo.long_block = e->tuning.long_mode == VD_LONG_BLOCK;
+  bo.pair_split = e->tuning.pair_split == 7 ? 7 : 6;
   return bo;
 }
 
@@ -350,7 +352,8 @@ struct HostChunk {
   bool any_long = false;           // a read longer than 32 (the robust tier strip-mines it)
   bool any_strip = false;          // a read longer than one 256-row strip (every tier strip-mines it)
   int64_t n_paired = 0;            // leading items that carry two reads (own kernels)
-  int64_t n_paired_wide = 0;       // the first of them, with 6-8 rows per lane
+  int64_t n_paired_wide = 0;       // the first of them, with pair_split..8 rows per lane
+  int pair_split = 6;              // rows per lane from which two-read items run at 12 warps per SM
   int64_t n_long = 0;              // the items after them: long reads, two haplotypes per item
   int long_R = kMaxR;              // rows per lane of those
   bool long_block = false;         // and their kernel: block per item (else warp per item)
@@ -699,7 +702,9 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
   auto mid = std::stable_partition(c.items.begin(), c.items.end(),
                                    [](const WorkItem& w) { return code_paired(w.code); });
   c.n_paired = (int64_t)(mid - c.items.begin());
-  auto wide = std::stable_partition(c.items.begin(), mid, [](const WorkItem& w) { return code_R(w.code) >= 6; });
+  c.pair_split = bo.pair_split;
+  auto wide = std::stable_partition(c.items.begin(), mid,
+                                    [&](const WorkItem& w) { return code_R(w.code) >= bo.pair_split; });
   c.n_paired_wide = (int64_t)(wide - c.items.begin());
   auto lend = std::stable_partition(mid, c.items.end(), [](const WorkItem& w) { return code_long(w.code); });
   c.n_long = (int64_t)(lend - mid);
@@ -988,7 +993,9 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       qp.items = (const WorkItem*)(d + L.o_items) + lo;
       qp.n_items = hi - lo;
       qp.head = cnt + 6 + k;
-      err = launch_pair_f32(k == 0, bv, qp, &dt->f32, ht->s32, e->grid_pair[k == 0 ? 1 : 0], pl->stream);
+      const int split = pl->chunk.pair_split;
+      err = launch_pair_f32(k == 0, split, bv, qp, &dt->f32, ht->s32, e->grid_pair[split == 7][k == 0 ? 1 : 0],
+                            pl->stream);
       if (err != cudaSuccess) return cuda_fail(err, "two-read tier launch");
       ++n;
     }
@@ -1119,12 +1126,13 @@ int init_engine_grids(vd_engine* e) {
     }
   int bps = 0;
   cudaError_t err = cudaSuccess;
-  for (int wide = 0; wide < 2; ++wide) {
-    bps = 0;
-    err = occupancy_pair_f32(wide != 0, &bps);
-    if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
-    e->grid_pair[wide] = std::max(1, bps) * e->sm_count;
-  }
+  for (int sp = 0; sp < 2; ++sp)
+    for (int wide = 0; wide < 2; ++wide) {
+      bps = 0;
+      err = occupancy_pair_f32(wide != 0, sp ? 7 : 6, &bps);
+      if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
+      e->grid_pair[sp][wide] = std::max(1, bps) * e->sm_count;
+    }
   bps = 0;
   err = occupancy_drift_f32(&bps);
   if (err != cudaSuccess) return cuda_fail(err, "occupancy query");
@@ -1304,7 +1312,9 @@ int vd_engine_set_tuning(vd_engine* e, const vd_tuning* t) {
   if (t->pipeline_gcells < 0) return fail(VD_EINVAL, "pipeline_gcells must be >= 0");
   if (t->long_mode != VD_LONG_WARP && t->long_mode != VD_LONG_SINGLE && t->long_mode != VD_LONG_BLOCK)
     return fail(VD_EINVAL, "long_mode must be VD_LONG_WARP, VD_LONG_SINGLE or VD_LONG_BLOCK");
-  for (int i = 0; i < 3; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  if (t->pair_split != 0 && t->pair_split != 6 && t->pair_split != 7)
+    return fail(VD_EINVAL, "pair_split must be 6 or 7 (0 = 6)");
+  for (int i = 0; i < 2; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
   std::lock_guard<std::mutex> lk(e->mu);
   e->tuning = *t;
   return VD_OK;

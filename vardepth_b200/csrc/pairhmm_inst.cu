@@ -36,18 +36,29 @@ cudaError_t VD_NAME(occupancy, VD_TNAME, VD_MNAME)(int* blocks_per_sm) {
 }
 
 #if !VD_FP64 && !VD_ANCH
-cudaError_t launch_pair_f32(bool wide, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
-                            const Scalars<float>& sc, int grid, cudaStream_t stream) {
-  if (wide) pairhmm_pair_kernel<6, 8, 3><<<grid, kWarpsPerBlock * kWarp, 0, stream>>>(bv, qv, tab, sc);
-  else pairhmm_pair_kernel<1, 5, 4><<<grid, kWarpsPerBlock * kWarp, 0, stream>>>(bv, qv, tab, sc);
+// Two tilings of the rows-per-lane range: split 6 runs 1-5 rows at 16 warps per
+// SM and 6-8 at 12; split 7 moves 6 rows to the 16-warp kernel (128 registers,
+// a few spills) -- the autotuner measures which is faster for a batch.
+cudaError_t launch_pair_f32(bool wide, int split, const BatchView& bv, const QueueView& qv,
+                            const Tables<float>* tab, const Scalars<float>& sc, int grid, cudaStream_t stream) {
+  const int threads = kWarpsPerBlock * kWarp;
+  if (split == 7) {
+    if (wide) pairhmm_pair_kernel<7, 8, 3><<<grid, threads, 0, stream>>>(bv, qv, tab, sc);
+    else pairhmm_pair_kernel<1, 6, 4><<<grid, threads, 0, stream>>>(bv, qv, tab, sc);
+  } else {
+    if (wide) pairhmm_pair_kernel<6, 8, 3><<<grid, threads, 0, stream>>>(bv, qv, tab, sc);
+    else pairhmm_pair_kernel<1, 5, 4><<<grid, threads, 0, stream>>>(bv, qv, tab, sc);
+  }
   return cudaGetLastError();
 }
 
-cudaError_t occupancy_pair_f32(bool wide, int* blocks_per_sm) {
-  return wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<6, 8, 3>,
-                                                              kWarpsPerBlock * kWarp, 0)
-              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<1, 5, 4>,
-                                                              kWarpsPerBlock * kWarp, 0);
+cudaError_t occupancy_pair_f32(bool wide, int split, int* blocks_per_sm) {
+  const int threads = kWarpsPerBlock * kWarp;
+  if (split == 7)
+    return wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<7, 8, 3>, threads, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<1, 6, 4>, threads, 0);
+  return wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<6, 8, 3>, threads, 0)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pairhmm_pair_kernel<1, 5, 4>, threads, 0);
 }
 #endif
 

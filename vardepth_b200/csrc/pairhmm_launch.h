@@ -10,10 +10,11 @@ cudaError_t launch_f64(bool anchored, const BatchView& bv, const QueueView& qv, 
                        const Scalars<double>& sc, int tier, int grid, cudaStream_t stream);
 cudaError_t occupancy_f32(bool anchored, int* blocks_per_sm);
 cudaError_t occupancy_f64(bool anchored, int* blocks_per_sm);
-// two-read items (FP32, semiglobal): wide = 6-8 rows per lane, else 1-5
-cudaError_t launch_pair_f32(bool wide, const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
-                            const Scalars<float>& sc, int grid, cudaStream_t stream);
-cudaError_t occupancy_pair_f32(bool wide, int* blocks_per_sm);
+// two-read items (FP32, semiglobal): wide = split..8 rows per lane (12 warps per SM), else
+// 1..split-1 (16 warps per SM); split is 6 or 7
+cudaError_t launch_pair_f32(bool wide, int split, const BatchView& bv, const QueueView& qv,
+                            const Tables<float>* tab, const Scalars<float>& sc, int grid, cudaStream_t stream);
+cudaError_t occupancy_pair_f32(bool wide, int split, int* blocks_per_sm);
 // the drift tier (FP32 semiglobal rescue with per-row power-of-two boosts)
 cudaError_t launch_drift_f32(const BatchView& bv, const QueueView& qv, const Tables<float>* tab,
                              const Scalars<float>& sc, int grid, cudaStream_t stream);

@@ -56,12 +56,13 @@ class VdStats(ctypes.Structure):
 
 class VdTuning(ctypes.Structure):
     _fields_ = [("long_read_rows", ctypes.c_int), ("pair_mask", ctypes.c_int), ("max_item_columns", ctypes.c_int),
-                ("pipeline_gcells", ctypes.c_int), ("long_mode", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("pipeline_gcells", ctypes.c_int), ("long_mode", ctypes.c_int), ("pair_split", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
     def as_dict(self) -> dict:
         return {"long_read_rows": self.long_read_rows, "pair_mask": self.pair_mask,
                 "max_item_columns": self.max_item_columns, "pipeline_gcells": self.pipeline_gcells,
-                "long_mode": self.long_mode}
+                "long_mode": self.long_mode, "pair_split": self.pair_split or 6}
 
 
 class VdGenotypeOptions(ctypes.Structure):
@@ -319,11 +320,12 @@ class Engine:
         return t.as_dict()
 
     def set_tuning(self, long_read_rows: int = 256, pair_mask: int = 0x1FE, max_item_columns: int = 0,
-                   pipeline_gcells: int = 0, long_mode: int = VD_LONG_WARP) -> None:
+                   pipeline_gcells: int = 0, long_mode: int = VD_LONG_WARP, pair_split: int = 6) -> None:
         t = VdTuning()
         t.long_read_rows, t.pair_mask, t.max_item_columns = int(long_read_rows), int(pair_mask), int(max_item_columns)
         t.pipeline_gcells = int(pipeline_gcells)
         t.long_mode = int(long_mode)
+        t.pair_split = int(pair_split)
         check(library().vd_engine_set_tuning(self.handle, ctypes.byref(t)), "vd_engine_set_tuning")
 
     def forward(self, packed: Packed, params: VdParams, out: np.ndarray | None = None):
