@@ -256,6 +256,21 @@ def test_pair_list_regrouping_gives_the_region_results():
     assert eng.last["pairs"] == len(pairs)
 
 
+def test_pair_kernel_tiles_agree():
+    """The two tilings of the packed two-read kernels (pair_split 6 and 7: which rows-per-lane
+    counts run at 12 or 16 warps per SM) run the same arithmetic: identical results."""
+    w = S.batched_regions(n_regions=40)
+    eng = native.Engine(0, 4096)
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    a = eng.forward(_packed(w), params)[0]
+    eng.set_tuning(pair_split=7)
+    assert eng.tuning()["pair_split"] == 7
+    np.testing.assert_array_equal(eng.forward(_packed(w), params)[0], a)
+    with pytest.raises(ValueError):
+        eng.set_tuning(pair_split=5)
+    eng.close()
+
+
 def test_pipelined_chunks_agree():
     """vd_forward's pipelined chunks (the first a quarter of the others, each chunk's
     primary tier ordered after the previous one's) give the single-chunk results bit for bit."""
