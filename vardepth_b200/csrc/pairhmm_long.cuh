@@ -18,11 +18,11 @@
 // emission (a match costs no multiply) and the boosts are undone exactly in
 // the final exponent.  B is measured as the read goes: strip s+1 takes the
 // decay strip s showed at its bottom (the exponent of its boundary maximum),
-// and a strip whose bottom leaves 2^-100 .. 2^100 is run again with B
+// and a strip whose bottom leaves 2^-120 .. 2^100 is run again with B
 // corrected by what it measured (its input boundary is kept: the warp's slot
 // holds two boundary buffers, one read and one written).  The first strip
-// has nothing to learn from, so its input starts at 2^100: one pass measures
-// any decay up to about 200 bits.  Strips are renormalised to 2^0 exactly at
+// has nothing to learn from, so its input starts at 2^120: one pass measures
+// any decay from 20 to 240 bits (an error-rich read's first strip included).  Strips are renormalised to 2^0 exactly at
 // their end, as the primary tier does.  A pair still out of range after
 // kLongTries runs of a strip goes to the drift and FP64 tiers.
 //
@@ -37,8 +37,9 @@
 namespace vd {
 
 constexpr int kLongTries = 6;       // runs of one strip before a half gives up
-constexpr int kLongWindow = 100;    // a strip bottom must end in 2^-100 .. 2^100
-constexpr int kLongStart = 100;     // the first strip's input, 2^100 (binary orders)
+constexpr int kLongFloor = -120;    // a strip bottom must end in 2^-120 .. 2^100 (the FP32
+constexpr int kLongCeil = 100;      // normal range, with room above for the interior)
+constexpr int kLongStart = 120;     // the first strip's input, 2^120 (binary orders)
 
 template <int R>
 struct LongRows {
@@ -80,11 +81,13 @@ __device__ __forceinline__ int long_exponent(double v) {
 // One work item: read w.read against haplotypes hap_begin and hap_begin + 1
 // (nhap = 2) or hap_begin alone (nhap = 1); outputs out_begin (+1).
 // `scratch` is the warp's slot: 2 * half float4 boundary records (half >= the
-// longest haplotype + 1); `ring` 32 float4 of shared memory per warp.
+// longest haplotype + 1); `ring` and `oring` 32 float4 each of shared memory
+// per warp (the boundary read, the boundary written).
 template <int R>
 __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv, const WorkItem w,
                                           const Tables<float>* __restrict__ tb, const Scalars<float> sc,
-                                          const int lane, float4* __restrict__ scratch, float4* __restrict__ ring) {
+                                          const int lane, float4* __restrict__ scratch, float4* __restrict__ ring,
+                                          float4* __restrict__ oring) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr double kLn2 = 0.6931471805599453094;
   constexpr int SR = kWarp * R;
@@ -158,64 +161,132 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
     double accx = 0.0, accy = 0.0;
     float bmx = 0.f, bmy = 0.f;
+    const bool lane0 = lane == 0;
     // boundary records of the strip above, staged through the warp's ring:
-    // every 32 steps each lane loads one record of the next 32 columns
+    // every 32 steps each lane loads one record of the next 32 columns, and
+    // at every step all lanes read the record of lane 0's column (a broadcast)
     float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
     auto load_window = [&](int base) -> float4 {
       const int p = base + lane;
       return (strip > 0 && p <= M) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     };
-    nxt = load_window(0);
-    const int steps = M + 1 + (kWarp - 1);
-    for (int t = 0; t < steps; ++t) {
-      if ((t & (kWarp - 1)) == 0) {
-        __syncwarp();
-        ring[lane] = nxt;
-        __syncwarp();
-        nxt = load_window(t + kWarp);
+    auto stage_window = [&](int t) {
+      __syncwarp();
+      ring[lane] = nxt;
+      __syncwarp();
+      nxt = load_window(t + kWarp);
+    };
+    // this strip's bottom rows: lane 31 lays each column's record into the
+    // warp's out-ring, and every 32 columns the warp writes them to the
+    // boundary buffer in one coalesced store and folds them into the maxima
+    int flushed = 0;  // columns below this are in the boundary buffer
+    auto flush_out = [&](int count) {
+      __syncwarp();
+      if (lane < count) {
+        const int p = flushed + lane;
+        const float4 rec = oring[lane];
+        dst[p] = rec;
+        if (p <= m1) bmx = fmaxf(bmx, fmaxf(rec.x, rec.y));
+        if (p <= m2) bmy = fmaxf(bmy, fmaxf(rec.z, rec.w));
       }
+      __syncwarp();
+      flushed += count;
+    };
+    // lane 31 moves its FP32 row sums into FP64 after its columns 8r+7
+    auto flush_acc = [&]() {
+      accx += (double)acc32.x;
+      accy += (double)acc32.y;
+      acc32 = make_float2(0.f, 0.f);
+    };
+    const float2 cin2 = make_float2(cin, cin);
+    // one step; STEADY: every lane inside both haplotypes at a column >= 1
+    auto step = [&](auto steady_tag, const int t) {
+      constexpr bool STEADY = decltype(steady_tag)::value;
       const int p = t - lane;  // this lane's column
       float2 u_in = shfl_up2(u_bot);
       float2 s_in = shfl_up2(rw.s[R - 1]);
-      if (lane == 0) {
-        if (strip == 0) {
-          u_in = make_float2(cin, cin);
-          s_in = u_in;
-        } else {
-          const float4 rec = ring[t & (kWarp - 1)];
-          s_in = make_float2(rec.x, rec.z);
-          u_in = make_float2(rec.y, rec.w);
-        }
+      float2 in_s = cin2, in_u = cin2;
+      if (strip > 0) {
+        const float4 rec = ring[t & (kWarp - 1)];
+        in_s = make_float2(rec.x, rec.z);
+        in_u = make_float2(rec.y, rec.w);
       }
+      u_in = lane0 ? in_u : u_in;
+      s_in = lane0 ? in_s : s_in;
       u_in = __fmul2_rn(u_in, bf);
       s_in = __fmul2_rn(s_in, bf);
-      const bool inside = p >= 0 && p <= M;
-      // column 0 has no base (kNeverBase never matches); past a haplotype's
-      // end its half reads that haplotype's last base (its columns are not used)
-      const uint32_t hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
-      const uint32_t hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
-      column_long<R>(rw, hbx, hby, p > 0 ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
-      if (p <= 0) {
+      bool inside = true;
+      uint32_t hbx, hby;
+      if (STEADY) {
+        hbx = hp1[p];
+        hby = hp2[p];
+      } else {
+        // column 0 has no base (kNeverBase never matches); past a haplotype's
+        // end its half reads that haplotype's last base (its columns are not used)
+        inside = p >= 0 && p <= M;
+        hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
+        hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
+      }
+      column_long<R>(rw, hbx, hby, (STEADY || p > 0) ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
+      if (!STEADY && p <= 0) {
         // column 0 (and the lanes not started yet): no diagonal, no deletions
 #pragma unroll
         for (int r = 0; r < R; ++r) rw.W[r] = make_float2(0.f, 0.f);
       }
       s_top = s_in;
-      if (lane == kWarp - 1 && inside) {
-        if (last) {
-          // the final row sums, flushed into FP64 after every column 8r+7
+      if (last) {
+        // the final row sums (lane 31's are the ones used)
+        if (STEADY) {
+          acc32 = __fadd2_rn(acc32, u_bot);
+        } else if (lane == kWarp - 1 && inside) {
           if (p <= m1) acc32.x += u_bot.x;
           if (p <= m2) acc32.y += u_bot.y;
-          if ((p & 7) == 7) {
-            accx += (double)acc32.x;
-            accy += (double)acc32.y;
-            acc32 = make_float2(0.f, 0.f);
-          }
-        } else {
-          dst[p] = make_float4(rw.s[R - 1].x, u_bot.x, rw.s[R - 1].y, u_bot.y);
-          if (p <= m1) bmx = fmaxf(bmx, fmaxf(rw.s[R - 1].x, u_bot.x));
-          if (p <= m2) bmy = fmaxf(bmy, fmaxf(rw.s[R - 1].y, u_bot.y));
+          if ((p & 7) == 7) flush_acc();
         }
+      } else if (lane == kWarp - 1 && inside) {
+        oring[p & (kWarp - 1)] = make_float4(rw.s[R - 1].x, u_bot.x, rw.s[R - 1].y, u_bot.y);
+      }
+    };
+    // the out-ring is full when lane 31 has finished column flushed + 31
+    auto maybe_flush = [&](int t) {
+      if (!last && t - (kWarp - 1) == flushed + kWarp - 1) flush_out(kWarp);
+    };
+
+    nxt = load_window(0);
+    const int steps = M + 1 + (kWarp - 1);
+    // steady steps: every lane at a column in 1 .. min(m1, m2)
+    const int t_lo = kWarp, t_hi = min(m1, m2) + 1;
+    int t = 0;
+    for (; t < steps && (t < t_lo || (t < t_hi && (t & 7) != 0)); ++t) {
+      if ((t & (kWarp - 1)) == 0) stage_window(t);
+      step(std::false_type{}, t);
+      maybe_flush(t);
+    }
+    // blocks of 8 steps start at a multiple of 8, so lane 31's columns 8r+7
+    // fall at the block's step 6 and its out-ring fills at step 6 of every
+    // fourth block
+    for (; t + 8 <= t_hi; t += 8) {
+      if ((t & (kWarp - 1)) == 0) stage_window(t);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        step(std::true_type{}, t + u);
+        if (u == 6) {
+          if (last) flush_acc();
+          else maybe_flush(t + u);
+        }
+      }
+    }
+    for (; t < steps; ++t) {
+      if ((t & (kWarp - 1)) == 0) stage_window(t);
+      step(std::false_type{}, t);
+      maybe_flush(t);
+    }
+    if (!last && flushed <= M) flush_out(M + 1 - flushed);
+    if (!last) {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        bmx = fmaxf(bmx, __shfl_xor_sync(FULL, bmx, o));
+        bmy = fmaxf(bmy, __shfl_xor_sync(FULL, bmy, o));
       }
     }
     __syncwarp();
@@ -225,8 +296,8 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
       lgx = long_exponent(zx);
       lgy = long_exponent(zy);
     } else {
-      lgx = long_exponent(__shfl_sync(FULL, bmx, kWarp - 1));
-      lgy = long_exponent(__shfl_sync(FULL, bmy, kWarp - 1));
+      lgx = long_exponent(bmx);
+      lgy = long_exponent(bmy);
     }
   };
 
@@ -237,8 +308,8 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     const int ns = min(SR, n - strip * SR);
     for (int attempt = 0;; ++attempt) {
       run_strip(strip, last);
-      const bool gx = !okx || (lgx >= -kLongWindow && lgx < kLongWindow);
-      const bool gy = !oky || (lgy >= -kLongWindow && lgy < kLongWindow);
+      const bool gx = !okx || (lgx >= kLongFloor && lgx < kLongCeil);
+      const bool gy = !oky || (lgy >= kLongFloor && lgy < kLongCeil);
       if (gx && gy) break;
       if (attempt + 1 == kLongTries) {
         if (!gx) { okx = false; fail_x = true; }
@@ -318,7 +389,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
 pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
                     const Scalars<float> sc) {
   __shared__ Tables<float> tab;
-  __shared__ float4 rings[kWarpsPerBlock][kWarp];
+  __shared__ float4 rings[kWarpsPerBlock][2][kWarp];
   {
     const int words = (int)(sizeof(Tables<float>) / sizeof(int));
     const int* src = reinterpret_cast<const int*>(gtab);
@@ -341,7 +412,8 @@ pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
       i = __shfl_sync(0xffffffffu, i, 0);
     }
     if ((long long)i >= qv.n_items) break;
-    process_long<R>(bv, qv, qv.items[i], &tab, sc, lane, scratch, rings[threadIdx.x >> 5]);
+    process_long<R>(bv, qv, qv.items[i], &tab, sc, lane, scratch, rings[threadIdx.x >> 5][0],
+                    rings[threadIdx.x >> 5][1]);
   }
 }
 
@@ -555,11 +627,11 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
       bool gx = !okx, gy = !oky;
       if (!gx) {
         gx = true;
-        for (int wi = 0; wi < active; ++wi) gx &= sh.lg[wi][0] >= -kLongWindow && sh.lg[wi][0] < kLongWindow;
+        for (int wi = 0; wi < active; ++wi) gx &= sh.lg[wi][0] >= kLongFloor && sh.lg[wi][0] < kLongCeil;
       }
       if (!gy) {
         gy = true;
-        for (int wi = 0; wi < active; ++wi) gy &= sh.lg[wi][1] >= -kLongWindow && sh.lg[wi][1] < kLongWindow;
+        for (int wi = 0; wi < active; ++wi) gy &= sh.lg[wi][1] >= kLongFloor && sh.lg[wi][1] < kLongCeil;
       }
       if (gx && gy) break;
       if (attempt + 1 == kLongTries) {
