@@ -447,6 +447,11 @@ def test_autotune_on_a_sample():
     assert {k: eng.tuning()[k] for k in autotune.DEFAULT} == {k: best[k] for k in autotune.DEFAULT}
     after, _ = eng.forward(_packed(w), params)
     assert_mixed_close(after, before)
+    # stratified: the long-read knobs on the long-read regions, the others on the short ones
+    log = []
+    best = autotune.autotune(eng, _packed(w), params, repeats=1, use_cache=False, log=log, stratify=True)
+    assert {t["sample"] for t in log} == {"long", "short"}
+    assert_mixed_close(eng.forward(_packed(w), params)[0], before)
     eng.close()
 
 
@@ -584,4 +589,25 @@ def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
         other = eng.forward(_packed(w), batched)[0]
         assert_mixed_close(other, want)
         np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], other)
+    eng.close()
+
+
+@pytest.mark.parametrize("mode", ["warp", "block", "single"])
+def test_error_rich_long_read_regions_every_long_path(mode):
+    """The mixed-length workload's long-read regions (2-8 reads of 1-10 kb at 6% substitution and
+    2% indel error, 2-32 haplotypes each): every long-read path within 1e-4 log10 of the FP64
+    oracle on every pair, with the genotype argmax unchanged."""
+    rng = np.random.default_rng(4242)
+    w = S._mixed_regions(rng, 600, S.GAP_Q45, S.EXT_Q10)
+    rl = np.diff(w.read_off)
+    longest = np.maximum.reduceat(rl, w.region_read_off[:-1])
+    sub = w.subset(np.flatnonzero(longest > 256)[:4])
+    want = _oracle_workload(sub)
+    eng = native.Engine(0, 8192)
+    eng.set_tuning(long_mode={"warp": native.VD_LONG_WARP, "block": native.VD_LONG_BLOCK,
+                              "single": native.VD_LONG_SINGLE}[mode])
+    params, _ = native.make_params(sub.gap, sub.ext, False, native.VD_PRECISION_MIXED)
+    got, _ = eng.forward(_packed(sub), params)
+    assert_mixed_close(got, want)
+    assert _argmax_agree(sub, got, want) == (sub.n_regions, sub.n_regions)
     eng.close()

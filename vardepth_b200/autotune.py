@@ -86,11 +86,56 @@ def _time(engine: native.Engine, packed: native.Packed, params, setting: dict, r
     return float(np.median(ms))
 
 
+LONG_KNOBS = ("long_mode", "long_read_rows")     # act on reads longer than one strip only
+SHORT_KNOBS = ("pair_split", "pair_mask", "max_item_columns")
+
+
+def split_samples(packed: native.Packed, fraction: float = 0.02, min_regions: int = 200, long_items: int = 8192,
+                  seed: int = 2024):
+    """Two seeded region samples of a region-form batch: regions holding a read longer than one
+    256-row strip ("long") and the others ("short").  The short sample is `fraction` of the short
+    regions (at least `min_regions`); the long sample takes long regions until it holds about
+    `long_items` read x haplotype-pair items, enough to fill every warp of the device several
+    times over, because the long kernels' time on a few long items is their slowest item's, not
+    their throughput.  Either may be None."""
+    from . import shard
+    rr, hh = packed.region_read_off, packed.region_hap_off
+    rl = np.diff(packed.read_off)
+    longest = np.zeros(len(rr) - 1, np.int64)
+    nz = np.diff(rr) > 0
+    longest[nz] = np.maximum.reduceat(rl, rr[:-1][nz])
+    is_long = longest > 256
+    rng = np.random.default_rng(seed)
+    out = []
+    short = np.flatnonzero(~is_long)
+    if len(short):
+        k = min(len(short), max(min_regions, int(round(fraction * len(short)))))
+        out.append(np.sort(rng.choice(short, size=k, replace=False)))
+    else:
+        out.append(None)
+    long_ = np.flatnonzero(is_long)
+    if len(long_):
+        order = rng.permutation(long_)
+        items = np.diff(rr)[order] * ((np.diff(hh)[order] + 1) // 2)
+        k = min(len(order), int(np.searchsorted(np.cumsum(items), long_items)) + 1)
+        out.append(np.sort(order[:k]))
+    else:
+        out.append(None)
+    return [None if g is None else shard.subset(packed, g)[0] for g in out]
+
+
 def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int = 3, use_cache: bool = True,
-             log: list | None = None) -> dict:
-    """Choose vd_tuning for this batch shape by timing candidates on ``packed`` (normally a sample
-    of the real batch); the best setting stays on the engine and is returned."""
-    key = f"{engine.info()['gpu']}|{signature(packed.read_off, packed.hap_off)}|anch={params.anchored}"
+             log: list | None = None, stratify: bool = False) -> dict:
+    """Choose vd_tuning for this batch shape by timing candidates and leave the best on the
+    engine.  With stratify=False ``packed`` is already the sample every knob is timed on; with
+    stratify=True it is the whole batch (region form) and the long-read knobs are timed on its
+    long-read regions, the others on a sample of its short-read regions (split_samples)."""
+    if stratify:
+        short_s, long_s = split_samples(packed)
+    else:
+        short_s, long_s = packed, packed
+    sig_src = packed
+    key = f"{engine.info()['gpu']}|{signature(sig_src.read_off, sig_src.hap_off)}|anch={params.anchored}"
     cache = {}
     if use_cache and CACHE.exists():
         try:
@@ -98,24 +143,32 @@ def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int 
         except (OSError, ValueError):
             cache = {}
     if use_cache and key in cache:
-        best = cache[key]
+        best = dict(DEFAULT, **cache[key])
         _apply(engine, best)
         return dict(best, cached=True)
     best = dict(DEFAULT)
-    best_ms = _time(engine, packed, params, best, repeats)
-    trials = [(dict(best), best_ms)]
-    for knob, values in SPACE.items():
-        for v in values:
-            if v == best[knob]:
-                continue
-            cand = dict(best, **{knob: v})
-            ms = _time(engine, packed, params, cand, repeats)
-            trials.append((cand, ms))
-            if ms < best_ms * 0.99:
-                best, best_ms = cand, ms
+    trials = []
+    default_ms = {}
+    sample_ms = {}
+    for knobs, sample, name in ((LONG_KNOBS, long_s, "long"), (SHORT_KNOBS, short_s, "short")):
+        if sample is None:
+            continue
+        best_ms = _time(engine, sample, params, best, repeats)
+        default_ms[name] = round(best_ms, 3)
+        trials.append((name, dict(best), best_ms))
+        for knob in knobs:
+            for v in SPACE[knob]:
+                if v == best[knob]:
+                    continue
+                cand = dict(best, **{knob: v})
+                ms = _time(engine, sample, params, cand, repeats)
+                trials.append((name, cand, ms))
+                if ms < best_ms * 0.99:
+                    best, best_ms = cand, ms
+        sample_ms[name] = round(best_ms, 3)
     _apply(engine, best)
     if log is not None:
-        log.extend({"setting": t, "ms": round(ms, 3)} for t, ms in trials)
+        log.extend({"sample": nm, "setting": t, "ms": round(ms, 3)} for nm, t, ms in trials)
     if use_cache:
         cache[key] = best
         try:
@@ -123,4 +176,6 @@ def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int 
             CACHE.write_text(json.dumps(cache, indent=1))
         except OSError:
             pass
-    return dict(best, sample_ms=round(best_ms, 3), default_ms=round(trials[0][1], 3), cached=False)
+    return dict(best, sample_ms=sample_ms, default_ms=default_ms, cached=False,
+                samples={k: (None if v is None else int(len(v.region_read_off) - 1))
+                         for k, v in (("short", short_s), ("long", long_s))})

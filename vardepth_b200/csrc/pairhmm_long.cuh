@@ -18,11 +18,12 @@
 // emission (a match costs no multiply) and the boosts are undone exactly in
 // the final exponent.  B is measured as the read goes: strip s+1 takes the
 // decay strip s showed at its bottom (the exponent of its boundary maximum),
-// and a strip whose bottom leaves 2^-120 .. 2^100 is run again with B
+// and a strip whose bottom leaves 2^-60 .. 2^60 is run again with B
 // corrected by what it measured (its input boundary is kept: the warp's slot
 // holds two boundary buffers, one read and one written).  The first strip
-// has nothing to learn from, so its input starts at 2^120: one pass measures
-// any decay from 20 to 240 bits (an error-rich read's first strip included).  Strips are renormalised to 2^0 exactly at
+// has nothing to learn from, so its input starts at 2^60: one pass takes any
+// decay up to 120 bits; an error-rich read's first strip (about 240) runs a
+// second time with the rate its first run measured.  Strips are renormalised to 2^0 exactly at
 // their end, as the primary tier does.  A pair still out of range after
 // kLongTries runs of a strip goes to the drift and FP64 tiers.
 //
@@ -37,9 +38,14 @@
 namespace vd {
 
 constexpr int kLongTries = 6;       // runs of one strip before a half gives up
-constexpr int kLongFloor = -120;    // a strip bottom must end in 2^-120 .. 2^100 (the FP32
-constexpr int kLongCeil = 100;      // normal range, with room above for the interior)
-constexpr int kLongStart = 120;     // the first strip's input, 2^120 (binary orders)
+// A strip bottom must end in 2^-60 .. 2^60: the cells that carry the mass lie
+// within a few dozen binary orders below the bottom's maximum, and they must
+// stay far above 2^-126, where the packed f32x2 arithmetic loses them (with
+// bottoms allowed down to 2^-100 the error reached 8e-4 log10 on 8%-error
+// 7 kb reads, down to 2^-120 0.1; at 2^-60 it stays at the FP32 rounding level)
+constexpr int kLongFloor = -60;
+constexpr int kLongCeil = 60;
+constexpr int kLongStart = 60;      // the first strip's input, 2^60 (binary orders)
 
 template <int R>
 struct LongRows {
@@ -640,23 +646,32 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
         break;
       }
       // each warp's rows get their own measured decay (in: the warp above's
-      // bottom, or the tall strip's input), aiming every bottom at 2^0; a warp
-      // whose bottom over- or underflowed steps by half a bit per row, one fed
-      // by such a warp waits for it
+      // bottom, or the tall strip's input), aiming every bottom at 2^0.  A
+      // warp whose bottom over- or underflowed, or whose input did, takes the
+      // decay rate (bits per row) measured by the lowest warp above it that
+      // could measure one, so a first tall strip converges in two or three
+      // runs rather than one warp per run
       __syncthreads();
       if (tid == 0) {
         for (int hf = 0; hf < 2; ++hf) {
           if (hf == 0 ? gx : gy) continue;
+          int rate_num = -1, rate_den = 1;  // last measured decay and its rows
+          bool input_ok = true;
           for (int wi = 0; wi < active; ++wi) {
             const int in = wi == 0 ? start : sh.lg[wi - 1][hf];
             const int lg = sh.lg[wi][hf];
             const int ns = rows_of(wi);
             int B = sh.B[wi][hf];
-            if (in == 1024 || in == -1024) break;
-            if (lg == 1024 || lg == -1024) {
+            input_ok = input_ok && in != 1024 && in != -1024;
+            if (input_ok && lg != 1024 && lg != -1024) {
+              const int d = B + in - lg;  // this warp's own decay
+              rate_num = d;
+              rate_den = ns;
+              B = d - (wi == 0 ? start : 0);
+            } else if (rate_num >= 0) {
+              B = rate_num * ns / rate_den - (wi == 0 ? start : 0);
+            } else if (input_ok) {
               B += lg == 1024 ? -ns / 2 : ns / 2;
-            } else {
-              B = B + in - lg - (wi == 0 ? start : 0);
             }
             sh.B[wi][hf] = max(-4 * ns, min(4 * ns, B));
           }
