@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
                     help="run vardepth_b200.autotune on a 2%% region sample first (auto: every forward workload)")
+    ap.add_argument("--long-mode", choices=["warp", "block", "single"], default=None,
+                    help="fix the long-read path (vd_tuning.long_mode) instead of autotuning it")
     ap.add_argument("--workload", default="batched_regions",
                     choices=["batched_regions", "long_haplotype_stress", "planted_error_model", "mixed_length_regions"],
                     help="batched_regions (default) is the metric's workload; the others print their own line")
@@ -487,7 +489,10 @@ def main():
 
     # ---- autotuner: work-list choices timed on region samples, kept on the engine ----
     tuned = None
-    if args.autotune == "on" or args.autotune == "auto":
+    if args.long_mode is not None:
+        engine.set_tuning(**dict(engine.tuning(), long_mode={"warp": native.VD_LONG_WARP, "block": native.VD_LONG_BLOCK,
+                                                             "single": native.VD_LONG_SINGLE}[args.long_mode]))
+    elif args.autotune == "on" or args.autotune == "auto":
         from vardepth_b200 import autotune
         tlog = []
         t0 = time.perf_counter()
