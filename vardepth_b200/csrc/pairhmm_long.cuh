@@ -16,16 +16,17 @@
 // lane L's share of B.  A boost on a lane's inputs scales the lane's rows and
 // everything below by an exact power of two, so the rows keep the one-sided
 // emission (a match costs no multiply) and the boosts are undone exactly in
-// the final exponent.  B is measured as the read goes: strip s+1 takes the
-// decay strip s showed at its bottom (the exponent of its boundary maximum),
-// and a strip whose bottom leaves 2^-60 .. 2^60 is run again with B
-// corrected by what it measured (its input boundary is kept: the warp's slot
-// holds two boundary buffers, one read and one written).  The first strip
-// has nothing to learn from, so its input starts at 2^60: one pass takes any
-// decay up to 120 bits; an error-rich read's first strip (about 240) runs a
-// second time with the rate its first run measured.  Strips are renormalised to 2^0 exactly at
-// their end, as the primary tier does.  A pair still out of range after
-// kLongTries runs of a strip goes to the drift and FP64 tiers.
+// the final exponent.  B is measured as the read goes: each strip's decay is
+// read off the exponent of its boundary maximum, strip s+1 takes the read's
+// mean decay rate so far times its rows, and a strip whose bottom leaves
+// 2^-60 .. 2^60 is run again with B corrected by what it measured (its input
+// boundary is kept: the warp's slot holds two boundary buffers, one read and
+// one written).  The first strip has nothing to learn from, so its input
+// starts at 2^60: one pass takes any decay up to 120 bits; an error-rich
+// read's first strip (about 240) runs again with a corrected rate.  Strips
+// are renormalised to 2^0 exactly at their end, as the primary tier does.  A
+// pair still out of range after kLongTries runs of a strip goes to the drift
+// and FP64 tiers.
 //
 // Every choice above depends on the pair's own data only (B, the re-runs of a
 // strip and its renormalisation are per half; a re-run caused by the other
@@ -121,6 +122,12 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
 
   // per half: boost bits of the current strip, total exponent, still in play
   int Bx = 0, By = 0, Ex = 0, Ey = 0;
+  // decay measured over the strips done so far (bits, rows): the next strip's
+  // boost is this mean rate times its rows.  A single strip's decay scatters
+  // by tens of bits around the read's rate (the number of errors in 256 rows),
+  // so the mean predicts the next strip about sqrt(2) times better than the
+  // last strip alone, and fewer strips run twice
+  int Dx = 0, Dy = 0, Nrows = 0;
   bool okx = true, oky = two;
   int lgx = 0, lgy = 0;        // bottom exponents of the last run
   double zx = 0.0, zy = 0.0;   // final sums (last strip, lane 31)
@@ -351,13 +358,16 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
       }
       __syncwarp();
       const int ns1 = min(SR, n - (strip + 1) * SR);
+      Nrows += ns;
       if (okx) {
         Ex += Bx + start + ksx;
-        Bx = max(0, min(4 * ns1, (Bx + start - lgx) * ns1 / ns));
+        Dx += Bx + start - lgx;
+        Bx = max(0, min(4 * ns1, Dx * ns1 / Nrows));
       }
       if (oky) {
         Ey += By + start + ksy;
-        By = max(0, min(4 * ns1, (By + start - lgy) * ns1 / ns));
+        Dy += By + start - lgy;
+        By = max(0, min(4 * ns1, Dy * ns1 / Nrows));
       }
     } else {
       Ex += Bx + start;
@@ -452,6 +462,8 @@ struct LongBlockShared {
   float4 ring0[kWarp];                          // warp 0: boundary records of the tall strip above
   int lg[kWarpsPerBlock][2];                    // bottom exponents of the last run
   int B[kWarpsPerBlock][2];                     // boost bits of each warp's rows
+  int D[2];                                     // decay (bits) over the rows done so far
+  int rows;                                     // those rows
   double z[2];                                  // final sums
   long long item;
 };
@@ -492,6 +504,8 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
   const float cin = sc.c * pow2T(kLongStart, 0.f);
 
   if (tid < NW * 2) sh.B[tid >> 1][tid & 1] = 0;
+  if (tid < 2) sh.D[tid] = 0;
+  if (tid == 0) sh.rows = 0;
   __syncthreads();
   // per half, identical in every thread: total exponent, still in play
   int Ex = 0, Ey = 0;
@@ -702,13 +716,15 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
       const int rows1 = min(H, n - (S + 1) * H);
       __syncthreads();
       if (tid == 0) {
+        // every warp of the next tall strip takes the read's mean decay rate
+        // so far (the decays of this tall strip's warps telescope to its
+        // boosts plus its input minus its bottom), times its rows
+        sh.rows += rows;
         for (int hf = 0; hf < 2; ++hf) {
+          sh.D[hf] += (hf == 0 ? sumBx : sumBy) + start - sh.lg[active - 1][hf];
           for (int wi = 0; wi < NW; ++wi) {
-            const int ns1 = min(SR, rows1 - wi * SR);
-            if (wi >= active || ns1 <= 0) { sh.B[wi][hf] = wi > 0 ? sh.B[wi - 1][hf] : 0; continue; }
-            const int in = wi == 0 ? start : sh.lg[wi - 1][hf];
-            const int d = sh.B[wi][hf] + in - sh.lg[wi][hf];
-            sh.B[wi][hf] = max(0, min(4 * ns1, d * ns1 / rows_of(wi)));
+            const int ns1 = max(0, min(SR, rows1 - wi * SR));
+            sh.B[wi][hf] = max(0, min(4 * ns1, (int)((long long)sh.D[hf] * ns1 / sh.rows)));
           }
         }
       }
