@@ -107,8 +107,8 @@ typedef struct vd_stats {
   double rescue_ms;         /* device time of the two FP64 rescue tiers */
   int64_t shared_cells;     /* of dp_cells, those of haplotype columns that repeat the previous
                                haplotype of the region and were not streamed again */
-  int64_t rescued_fp32;     /* pairs the primary tier spilled that the FP32 drift tier (reads
-                               longer than 256 bases, per-row power-of-two boosts) resolved */
+  int64_t rescued_fp32;     /* pairs the primary tier spilled that the FP32 drift tier (per-row
+                               power-of-two boosts, semiglobal) resolved */
 } vd_stats;
 
 typedef struct vd_engine vd_engine;

@@ -550,6 +550,37 @@ def test_drift_tier_error_rich_long_reads():
     eng.close()
 
 
+def test_drift_tier_one_strip_reads_below_the_fp32_range():
+    """Reads of one strip (40-256 bases) carrying 8-36 Q40 mismatches against every
+    haplotype: likelihoods 2^-120 .. 2^-540 below a perfect match, many under the primary
+    tier's FP32 range.  The drift tier rescores them in FP32 with one boost per read, within
+    1e-4 log10 of the FP64 oracle, bit-identical under the plain schedule, with none left to FP64."""
+    rng = np.random.default_rng(77)
+    regions = []
+    for n in (40, 100, 150, 200, 256):
+        hap0 = S._random_hap(rng, 420)
+        haps = [hap0, S._mutate(rng, hap0, 2, 4)]
+        reads, quals = [], []
+        for k in range(8, 37, 4):
+            a = int(rng.integers(0, 420 - n))
+            r = hap0[a:a + n].copy()
+            for p in rng.choice(n, size=min(k, n - 1), replace=False):
+                r[p] = S.ALPHABET[S.ALPHABET != r[p]][rng.integers(0, 3)]
+            reads.append(r)
+            quals.append(np.full(n, 40, np.uint8))
+        regions.append((haps, reads, quals))
+    w = S._assemble("one-strip drift", regions, S.GAP_Q45, S.EXT_Q10, {})
+    want = _oracle_workload(w)
+    eng = native.Engine(0, 4096)
+    batched, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    plain, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED, schedule=native.VD_SCHEDULE_PLAIN)
+    got, st = eng.forward(_packed(w), batched)
+    assert st.rescued_fp32 >= 20 and st.rescued_fp64 + st.rescued_robust == 0
+    assert_mixed_close(got, want)
+    np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], got)
+    eng.close()
+
+
 def _long_read_regions(seed, lengths, err, n_haps):
     """One region per read length: n_haps haplotypes (a base and edited copies of unequal
     lengths) and two reads of that length at substitution rate err (indels err / 4)."""

@@ -93,15 +93,18 @@ __device__ __forceinline__ void spill_pair(const QueueView& qv, int32_t read, in
 
 constexpr int kUnroll = 8;
 
-// The drift tier (FP32, semiglobal, reads longer than one strip) rescores the
-// pairs the primary tier spilled.  Error-rich long reads lose more per strip
+// The drift tier (FP32, semiglobal) rescores the pairs the primary tier
+// spilled.  Error-rich long reads lose more per strip
 // than the FP32 range holds (8% errors at reported Q30: about 1 bit per row),
 // so each row's constants are multiplied by an exact power of two 2^k_i that
 // cancels the decay: Bs bits per strip, spread over its rows.  Bs is measured
 // as the read goes (the next strip takes the decay left over at the bottom of
 // this one) and a strip whose bottom leaves the window [2^-60, 2^60) is run
 // again with Bs corrected by the measured exponent (its input boundary is kept
-// in the other half of the warp's scratch).  What still fails goes to FP64.
+// in the other half of the warp's scratch).  A read of one strip spilled
+// because its likelihood lies below the primary tier's range; its lanes each
+// take their own boost, measured lane by lane (a variant or a cluster of
+// errors concentrates the decay in a few rows).  What still fails goes to FP64.
 constexpr int kDriftTries = 6;
 
 // Row layout of one read (lane L, register r of strip s holds row
@@ -159,6 +162,11 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   const long long half = drift ? qv.scratch_stride / 2 : qv.scratch_stride;
   int strip_lg = 0;     // drift: exponent of the strip's bottom maximum (or +-1024: inf / zero)
   double zkeep = 0.0;   // drift: the last strip's final sum, on lane 31
+  // drift, reads of one strip: each lane's own boost bits (spread over its read
+  // rows) and the maximum of its bottom row's u over the columns of the last run
+  bool lane_boost = false;
+  int kl_lane = 0;
+  T lmax_keep = T(0);
 
   // One strip of rows (Bs: the drift tier's boost bits for the strip, else 0).
   // FIRST and LAST are compile-time tags, so the steady loop carries no
@@ -187,9 +195,13 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
         rw.X[r] = (!ANCH && i == n - 1) ? A : tb->X[q];
         if constexpr (kCanDrift) {
           {
-            // row il of the strip gets k = floor((il+1) Bs / ns) - floor(il Bs / ns)
+            // row il of the strip gets k = floor((il+1) Bs / ns) - floor(il Bs / ns),
+            // or its share of the lane's own boost (the lane's read rows split it)
             const int il = i - strip * SR;
-            const T f = pow2T((il + 1) * Bs / ns - il * Bs / ns, T(0));
+            const int lrows = min(R, n - lane * R);
+            const int kr = lane_boost ? (r + 1) * kl_lane / lrows - r * kl_lane / lrows
+                                      : (il + 1) * Bs / ns - il * Bs / ns;
+            const T f = pow2T(kr, T(0));
             rw.miss[r] *= f;
             rw.hit[r] *= f;
             rw.K[r] *= f;
@@ -216,6 +228,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
     const uint8_t* hp = bv.hap_bases;  // hp[p] = haplotype base at stream position p
     T s_top = T(0), u_bot = T(0);
     T acc32 = T(0), cap = T(0), rmax = T(0), bmax = T(0);
+    T lmax = T(0);  // drift: maximum of this lane's bottom-row u
     double acc64 = 0.0;
 
     auto finalize = [&](int k) {
@@ -334,6 +347,9 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       s_in = lane0 ? is : s_in;
       T tmu = T(0), tnu = T(0), tom = T(0);
       column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
+      if constexpr (drift) {
+        if (active) lmax = maxT(lmax, u_bot);
+      }
       s_top = s_in;
       if (last) {
         accumulate(tmu, tnu, tom);
@@ -366,6 +382,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       s_in = lane0 ? is : s_in;
       T tmu = T(0), tnu = T(0), tom = T(0);
       column<T, R, GEN, ANCH>(rw, hb, s_top, u_in, k2, x, u_bot, tmu, tnu, tom);
+      if constexpr (drift) lmax = maxT(lmax, u_bot);
       s_top = s_in;
       if (last) {
         accumulate(tmu, tnu, tom);
@@ -407,6 +424,7 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
       }
       S = Snext;
     }
+    if constexpr (drift) lmax_keep = lmax;
 
     if (!last) {
       // renormalise the boundary the next strip starts from: its maximum is
@@ -436,9 +454,61 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
   };
 
   if constexpr (drift) {
-    // rescue entries carry one haplotype; single-strip reads go on to FP64
-    bool ok = nstrips > 1 && K == 1;
-    if constexpr (R == kMaxR || R == 4 || R == 2 || R == 1) {
+    // rescue entries carry one haplotype
+    bool ok = K == 1;
+    if (nstrips == 1) {
+      // a read of one strip: the primary tier (row 0 at 2^120) spilled it because
+      // its final sum fell below 2^-80, so it decays by more than 200 bits.  Each
+      // lane boosts its own read rows.  The first run spreads 232 bits (32 above
+      // that bound) evenly over the read; a run is kept when every lane's
+      // bottom-row maximum and the final sum lie in 2^-60 .. 2^60.  Otherwise
+      // each lane takes the decay it measured (its boost plus its input's
+      // exponent minus its bottom's), so the next run holds every lane near 2^0
+      // wherever the read's errors sit.  The first lane whose bottom under- or
+      // overflowed moves by the bound that shows (149 bits: a nonzero float would
+      // have been seen), and the lanes below it take the mean rate of the lanes
+      // above.
+      const int used = (n + R - 1) / R;  // lanes holding read rows
+      const int lrows = lane < used ? min(R, n - lane * R) : 0;
+      const int B0 = min(16 * n, 232);
+      lane_boost = true;
+      kl_lane = lane < used ? (lane * R + lrows) * B0 / n - (lane * R) * B0 / n : 0;
+      for (int attempt = 0; ok; ++attempt) {
+        run_strip(std::true_type{}, std::true_type{}, 0, 0);
+        const double z = __shfl_sync(FULL, zkeep, kWarp - 1);
+        const T lm = lmax_keep;
+        const int lgl = lane >= used ? 0 : (lm != lm || lm >= T(HUGE_VAL)) ? 1024 : (lm > T(0) ? ilogb(lm) : -1024);
+        const bool in_window = lgl >= -60 && lgl < 60;
+        if (__all_sync(FULL, in_window) && z >= (double)sc.final_floor && z < (double)sc.strip_ceil) break;
+        if (attempt + 1 == kDriftTries) { ok = false; break; }
+        int in = __shfl_up_sync(FULL, lgl, 1);
+        if (lane == 0) in = 0;  // row 0 (c = 1)
+        const bool measured = lgl > -1024 && lgl < 1024;
+        const unsigned bad = __ballot_sync(FULL, lane < used && !measured);
+        const int first_bad = bad ? __ffs(bad) - 1 : kWarp;
+        const bool valid = lane < used && lane < first_bad;
+        const int d = valid ? kl_lane + in - lgl : 0;
+        int sum_d = d, sum_r = valid ? lrows : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+          sum_d += __shfl_xor_sync(FULL, sum_d, o);
+          sum_r += __shfl_xor_sync(FULL, sum_r, o);
+        }
+        int k = kl_lane;
+        if (valid) {
+          k = d;
+        } else if (lane < used) {
+          if (sum_r > 0) k = (int)((long long)sum_d * lrows / sum_r);
+          if (lane == first_bad) k = lgl == -1024 ? max(k, kl_lane + in + 149) : min(k, kl_lane + in - 128);
+        }
+        kl_lane = max(-24 * lrows, min(24 * lrows, k));
+      }
+      if (ok) {
+        E = kl_lane;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) E += __shfl_xor_sync(FULL, E, o);
+      }
+    } else if constexpr (R == kMaxR || R == 4 || R == 2 || R == 1) {
       int Bs = SR;  // first guess: one bit per row (the spilled reads lost more than 160 per strip)
       for (int strip = 0; ok && strip < nstrips; ++strip) {
         const int ns = min(SR, n - strip * SR);
@@ -473,13 +543,13 @@ __device__ __noinline__ void process_item(const BatchView bv, const QueueView qv
           Bs = max(0, min(16 * ns, Bs + (step != 0 ? step : (excess > 0 ? -1 : 1))));
         }
       }
-      if (ok && lane == kWarp - 1) {
-        const int64_t h = hap_index(0);
-        const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
-        bv.out[out_index(0)] = log(zkeep) - (sc.ln_c + log((double)(m + 1))) + lnN - (double)E * kLn2;
-      }
     } else {
       ok = false;  // no strip-mined variant at this R: the pair goes on to FP64
+    }
+    if (ok && lane == kWarp - 1) {
+      const int64_t h = hap_index(0);
+      const int m = (int)(bv.hap_off[h + 1] - bv.hap_off[h]);
+      bv.out[out_index(0)] = log(zkeep) - (sc.ln_c + log((double)(m + 1))) + lnN - (double)E * kLn2;
     }
     fail = !ok;
   } else if (nstrips == 1) {
@@ -976,8 +1046,8 @@ pairhmm_pair_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
 // on its own kernel so the strip driver's state does not crowd the primary
 // kernel's registers (launched with 4 blocks per SM, 128 registers: 7% faster
 // on the mixed-length workload's long reads than 3 blocks at 162 registers without spills).
-// Entries whose rows per lane have no strip-mined variant go on to FP64
-// unchanged.
+// Reads of one strip run at their own rows per lane; longer reads whose rows
+// per lane have no strip-mined variant go on to FP64 unchanged.
 template <int kBlocks>
 __global__ void __launch_bounds__(kWarpsPerBlock * kWarp, kBlocks)
 pairhmm_drift_kernel(const BatchView bv, const QueueView qv, const Tables<float>* __restrict__ gtab,
@@ -1013,10 +1083,10 @@ pairhmm_drift_kernel(const BatchView bv, const QueueView qv, const Tables<float>
     it.w.out2_begin = 0;
     it.w.code = bv.read_code[e.read];
     switch (code_R(it.w.code)) {
-      case 8: process_item<float, 8, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
-      case 4: process_item<float, 4, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
-      case 2: process_item<float, 2, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
-      case 1: process_item<float, 1, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
+#define VD_DCASE(r) \
+      case r: process_item<float, r, true, false, true>(bv, qv, it, &tab, sc, lane, scratch); break;
+      VD_DCASE(1) VD_DCASE(2) VD_DCASE(3) VD_DCASE(4) VD_DCASE(5) VD_DCASE(6) VD_DCASE(7) VD_DCASE(8)
+#undef VD_DCASE
       default:
         if (lane == 0) spill_pair<float>(qv, e.read, e.hap, e.out);
         __syncwarp();

@@ -23,9 +23,9 @@
 // boundary is kept: the warp's slot holds two boundary buffers, one read and
 // one written).  The first strip has nothing to learn from, so its input
 // starts at 2^60: one pass takes any decay up to 120 bits; an error-rich
-// read's first strip (about 240) runs again with a corrected rate.  Strips
-// are renormalised to 2^0 exactly at their end, as the primary tier does.  A
-// pair still out of range after kLongTries runs of a strip goes to the drift
+// read's first strip (about 240) runs again with a corrected rate.  A
+// strip's boundary is stored as computed and brought to 2^0 by an exact power
+// of two as the next strip loads it.  A pair still out of range after kLongTries runs of a strip goes to the drift
 // and FP64 tiers.
 //
 // Every choice above depends on the pair's own data only (B, the re-runs of a
@@ -50,11 +50,26 @@ constexpr int kLongStart = 60;      // the first strip's input, 2^60 (binary ord
 
 template <int R>
 struct LongRows {
-  uint32_t rb[R];     // read bases (kNeverBase for rows past the read)
-  float miss[R];      // mismatch factor of the row (the same for both halves)
-  float2 K[R], X[R];  // k1 f_i and (x/4) f_i (alpha f_n on the last row), both halves
-  float2 W[R], s[R];  // om of the next column and s of the column finished last
+  uint32_t rb[R];        // read bases (kNeverBase for rows past the read)
+  float miss[R];         // mismatch factor of rows 1 .. R-1 (the same for both halves)
+  float2 hit0, miss0;    // row 0's match and mismatch factors times the lane's boost, per half
+  float2 K[R], X[R];     // k1 f_i and (x/4) f_i (alpha f_n on the last row), both halves
+                         // (row 0's times the lane's boost)
+  float2 W[R], s[R];     // om of the next column and s of the column finished last
 };
+
+// The lane's boost 2^k multiplies every term that row 0 takes from above (the
+// diagonal s and the vertical u), so it is folded into row 0's factors once
+// per strip instead of into the two inputs at every step: the products are
+// the same bits (a power of two times a normal float is exact) and the
+// vertical chain through the lane's rows is one multiply shorter.
+template <int R>
+__device__ __forceinline__ void boost_row0(LongRows<R>& w, const float2 bf) {
+  w.hit0 = bf;
+  w.miss0 = make_float2(w.miss[0] * bf.x, w.miss[0] * bf.y);
+  w.K[0] = __fmul2_rn(w.K[0], bf);
+  w.X[0] = __fmul2_rn(w.X[0], bf);
+}
 
 template <int R>
 __device__ __forceinline__ void column_long(LongRows<R>& w, uint32_t hbx, uint32_t hby, float2 s_top, float2 u_top,
@@ -63,9 +78,16 @@ __device__ __forceinline__ void column_long(LongRows<R>& w, uint32_t hbx, uint32
   float2 nu = u_top;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    float2 mu_new = s_above;
-    mul_if_ne(mu_new.x, w.rb[r], hbx, w.miss[r]);
-    mul_if_ne(mu_new.y, w.rb[r], hby, w.miss[r]);
+    float2 mu_new;
+    if (r == 0) {
+      const float fx = w.rb[0] == hbx ? w.hit0.x : w.miss0.x;
+      const float fy = w.rb[0] == hby ? w.hit0.y : w.miss0.y;
+      mu_new = __fmul2_rn(s_above, make_float2(fx, fy));
+    } else {
+      mu_new = s_above;
+      mul_if_ne(mu_new.x, w.rb[r], hbx, w.miss[r]);
+      mul_if_ne(mu_new.y, w.rb[r], hby, w.miss[r]);
+    }
     const float2 om_new = w.W[r];
     const float2 u_new = __ffma2_rn(w.X[r], nu, mu_new);
     const float2 s_new = __ffma2_rn(k2, om_new, __ffma2_rn(w.K[r], nu, mu_new));
@@ -129,6 +151,7 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   // last strip alone, and fewer strips run twice
   int Dx = 0, Dy = 0, Nrows = 0;
   bool okx = true, oky = two;
+  int inx = 0, iny = 0;        // shifts that bring the boundary above to 2^0, per half
   int lgx = 0, lgy = 0;        // bottom exponents of the last run
   double zx = 0.0, zy = 0.0;   // final sums (last strip, lane 31)
 
@@ -166,10 +189,13 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
       kx = (lane + 1) * Bx / lanes_used - lane * Bx / lanes_used;
       ky = (lane + 1) * By / lanes_used - lane * By / lanes_used;
     }
-    const float2 bf = make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f));
+    boost_row0(rw, make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f)));
     const float cin = c0 * pow2T(kLongStart, 0.f);  // the first strip's row-0 value
     float4* const src = scratch + (long long)(strip & 1) * half;
     float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
+    // the boundary above is stored as written (its maximum at 2^lg); it is
+    // brought to 2^0 as it is loaded, by 2^-lg per half
+    const float fsx = pow2T(inx, 0.f), fsy = pow2T(iny, 0.f);
 
     float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
     double accx = 0.0, accy = 0.0;
@@ -181,7 +207,9 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
     auto load_window = [&](int base) -> float4 {
       const int p = base + lane;
-      return (strip > 0 && p <= M) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (strip == 0 || p > M) return make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 v = src[p];
+      return make_float4(v.x * fsx, v.y * fsx, v.z * fsy, v.w * fsy);
     };
     auto stage_window = [&](int t) {
       __syncwarp();
@@ -226,8 +254,6 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
       }
       u_in = lane0 ? in_u : u_in;
       s_in = lane0 ? in_s : s_in;
-      u_in = __fmul2_rn(u_in, bf);
-      s_in = __fmul2_rn(s_in, bf);
       bool inside = true;
       uint32_t hbx, hby;
       if (STEADY) {
@@ -341,22 +367,11 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     // the boosts of the strip count into the exponent (plus the first strip's start)
     const int start = strip == 0 ? kLongStart : 0;
     if (!last) {
-      // renormalise the boundary the next strip reads to 2^0 (two exact factors
-      // each, so any shift stays representable); the next strip's boost is this
-      // strip's decay, scaled to its rows
-      float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
+      // the next strip reads this one's boundary brought to 2^0 (|lg| <= 60, so
+      // one exact factor); its boost is this strip's decay, scaled to its rows
       const int ksx = okx ? -lgx : 0, ksy = oky ? -lgy : 0;
-      const float fx1 = pow2T(ksx / 2, 0.f), fx2 = pow2T(ksx - ksx / 2, 0.f);
-      const float fy1 = pow2T(ksy / 2, 0.f), fy2 = pow2T(ksy - ksy / 2, 0.f);
-      for (int p = lane; p <= M; p += kWarp) {
-        float4 v = dst[p];
-        v.x = (v.x * fx1) * fx2;
-        v.y = (v.y * fx1) * fx2;
-        v.z = (v.z * fy1) * fy2;
-        v.w = (v.w * fy1) * fy2;
-        dst[p] = v;
-      }
-      __syncwarp();
+      inx = ksx;
+      iny = ksy;
       const int ns1 = min(SR, n - (strip + 1) * SR);
       Nrows += ns;
       if (okx) {
@@ -448,8 +463,8 @@ pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
 // kLongRing >= kLongChunk + kLongLag columns).  Every warp takes the same
 // number of chunks and barriers whatever its share of the strip, so the
 // barriers always complete.  Each warp has its own boost rate (the decay of
-// its own rows, measured at its bottom), the tall strip is renormalised
-// exactly at its end, and a tall strip whose warps' bottoms leave the window
+// its own rows, measured at its bottom), the tall strip's boundary is brought
+// to 2^0 exactly as the next tall strip loads it, and a tall strip whose warps' bottoms leave the window
 // is run again with each warp's rate corrected by what it measured.
 constexpr int kLongChunk = 32;
 constexpr int kLongLag = 64;
@@ -510,6 +525,7 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
   // per half, identical in every thread: total exponent, still in play
   int Ex = 0, Ey = 0;
   bool okx = true, oky = two;
+  int inx = 0, iny = 0;  // shifts that bring the boundary above to 2^0, per half
 
   // one run of tall strip S; the warps' bottom exponents (or the final sums) land in sh
   auto run_tall = [&](const int S, const int active, const bool last) {
@@ -542,9 +558,11 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
       kx = (lane + 1) * Bx / lanes_used - lane * Bx / lanes_used;
       ky = (lane + 1) * By / lanes_used - lane * By / lanes_used;
     }
-    const float2 bf = make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f));
+    boost_row0(rw, make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f)));
     float4* const src = scratch + (long long)(S & 1) * half;
     float4* const dst = scratch + (long long)((S + 1) & 1) * half;
+    // the tall strip above's boundary, brought to 2^0 as warp 0 loads it
+    const float fsx = pow2T(inx, 0.f), fsy = pow2T(iny, 0.f);
     const bool bottom = wid == active - 1;  // this warp's bottom row is the tall strip's
     float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
     double accx = 0.0, accy = 0.0;
@@ -552,7 +570,9 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
     float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
     auto load_window = [&](int base) -> float4 {
       const int p = base + lane;
-      return (S > 0 && p <= M) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (S == 0 || p > M) return make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 v = src[p];
+      return make_float4(v.x * fsx, v.y * fsx, v.z * fsy, v.w * fsy);
     };
     if (wid == 0) nxt = load_window(0);
     for (int k = 0; k < chunks; ++k) {
@@ -582,8 +602,6 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
             u_in = make_float2(rec.y, rec.w);
           }
         }
-        u_in = __fmul2_rn(u_in, bf);
-        s_in = __fmul2_rn(s_in, bf);
         const bool inside = p >= 0 && p <= M;
         const uint32_t hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
         const uint32_t hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
@@ -693,24 +711,15 @@ __device__ __noinline__ void process_long_block(const BatchView bv, const QueueV
       }
       __syncthreads();
     }
-    // exponent bookkeeping, the renormalisation of the boundary and the rates
+    // exponent bookkeeping, the shift of the boundary and the rates
     // of the next tall strip (each warp's decay, scaled to its next rows)
     const int lgb_x = sh.lg[active - 1][0], lgb_y = sh.lg[active - 1][1];
     int sumBx = 0, sumBy = 0;
     for (int wi = 0; wi < active; ++wi) { sumBx += sh.B[wi][0]; sumBy += sh.B[wi][1]; }
     if (!last) {
       const int ksx = okx ? -lgb_x : 0, ksy = oky ? -lgb_y : 0;
-      float4* const dst = scratch + (long long)((S + 1) & 1) * half;
-      const float fx1 = pow2T(ksx / 2, 0.f), fx2 = pow2T(ksx - ksx / 2, 0.f);
-      const float fy1 = pow2T(ksy / 2, 0.f), fy2 = pow2T(ksy - ksy / 2, 0.f);
-      for (int p = tid; p <= M; p += NW * kWarp) {
-        float4 v = dst[p];
-        v.x = (v.x * fx1) * fx2;
-        v.y = (v.y * fx1) * fx2;
-        v.z = (v.z * fy1) * fy2;
-        v.w = (v.w * fy1) * fy2;
-        dst[p] = v;
-      }
+      inx = ksx;
+      iny = ksy;
       if (okx) Ex += sumBx + start + ksx;
       if (oky) Ey += sumBy + start + ksy;
       const int rows1 = min(H, n - (S + 1) * H);
