@@ -107,6 +107,45 @@ __device__ __forceinline__ int long_exponent(double v) {
   return (v != v || v >= HUGE_VAL) ? 1024 : (v > 0.0 ? ilogb(v) : -1024);
 }
 
+// One half's lane boosts after a run of a strip that left the window.  Lane
+// L measured the maximum of its bottom row (exponent lg_L, +-1024 for inf or
+// zero); with its input at 2^lg_{L-1} (lane 0: the strip's input, 2^in0) and
+// boost k_L, its rows decayed by d_L = k_L + lg_{L-1} - lg_L bits, and the
+// boost d_L (lane 0: d_0 - in0) brings its bottom to 2^0 wherever in the
+// strip the read's errors sit.  The first lane whose bottom under- or
+// overflowed moves by the bound that shows (a nonzero float lies above
+// 2^-149, a finite one below 2^128), and the lanes below it, whose inputs
+// are unknown, take the mean rate of the lanes above.  Shares stay within
+// -96 .. 120 bits, where 2^k times every row factor is a normal float.
+__device__ __forceinline__ int relane(const int kl, const float lm, const int used, const int lrows, const int in0,
+                                      const int lane) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lg = lane < used ? long_exponent(lm) : 0;
+  int in = __shfl_up_sync(FULL, lg, 1);
+  if (lane == 0) in = in0;
+  const int tgt = lane == 0 ? in0 : 0;  // the input the next run's lane sees
+  const bool measured = lg > -1024 && lg < 1024;
+  const unsigned bad = __ballot_sync(FULL, lane < used && !measured);
+  const int first_bad = bad ? __ffs(bad) - 1 : kWarp;
+  const bool valid = lane < used && lane < first_bad;
+  const int d = valid ? kl + in - lg : 0;
+  int sum_d = d, sum_r = valid ? lrows : 0;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    sum_d += __shfl_xor_sync(FULL, sum_d, o);
+    sum_r += __shfl_xor_sync(FULL, sum_r, o);
+  }
+  if (lane >= used) return 0;
+  int k = kl;
+  if (valid) {
+    k = d - tgt;
+  } else {
+    if (sum_r > 0) k = (int)((long long)sum_d * lrows / sum_r) - tgt;
+    if (lane == first_bad) k = lg == -1024 ? max(k, kl + in + 149 - tgt) : min(k, kl + in - 128 - tgt);
+  }
+  return max(-96, min(120, k));
+}
+
 // One work item: read w.read against haplotypes hap_begin and hap_begin + 1
 // (nhap = 2) or hap_begin alone (nhap = 1); outputs out_begin (+1).
 // `scratch` is the warp's slot: 2 * half float4 boundary records (half >= the
@@ -154,6 +193,8 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   int inx = 0, iny = 0;        // shifts that bring the boundary above to 2^0, per half
   int lgx = 0, lgy = 0;        // bottom exponents of the last run
   double zx = 0.0, zy = 0.0;   // final sums (last strip, lane 31)
+  int klx = 0, kly = 0;        // this lane's share of the strip's boost, per half
+  float lmx = 0.f, lmy = 0.f;  // this lane's bottom-row maxima in the last run
 
   // One run of strip `strip` with Bx / By boost bits; reads boundary buffer
   // src_half, writes the other.  Sets lgx / lgy (bottom maximum or final sum).
@@ -184,12 +225,7 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     // lane L's share of the boost: floor((L+1) B / lanes) - floor(L B / lanes)
     // over the lanes holding read rows; the first strip's input starts at 2^kLongStart
     // (|B| <= 4 ns keeps every share within +-4R, far inside the float exponent range)
-    int kx = 0, ky = 0;
-    if (lane < lanes_used) {
-      kx = (lane + 1) * Bx / lanes_used - lane * Bx / lanes_used;
-      ky = (lane + 1) * By / lanes_used - lane * By / lanes_used;
-    }
-    boost_row0(rw, make_float2(pow2T(kx, 0.f), pow2T(ky, 0.f)));
+    boost_row0(rw, make_float2(pow2T(klx, 0.f), pow2T(kly, 0.f)));
     const float cin = c0 * pow2T(kLongStart, 0.f);  // the first strip's row-0 value
     float4* const src = scratch + (long long)(strip & 1) * half;
     float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
@@ -200,6 +236,7 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
     double accx = 0.0, accy = 0.0;
     float bmx = 0.f, bmy = 0.f;
+    float2 lm = make_float2(0.f, 0.f);  // this lane's bottom-row maxima
     const bool lane0 = lane == 0;
     // boundary records of the strip above, staged through the warp's ring:
     // every 32 steps each lane loads one record of the next 32 columns, and
@@ -267,6 +304,13 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
         hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
       }
       column_long<R>(rw, hbx, hby, (STEADY || p > 0) ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
+      if (STEADY) {
+        lm.x = fmaxf(lm.x, u_bot.x);
+        lm.y = fmaxf(lm.y, u_bot.y);
+      } else {
+        if (inside && p <= m1) lm.x = fmaxf(lm.x, u_bot.x);
+        if (inside && p <= m2) lm.y = fmaxf(lm.y, u_bot.y);
+      }
       if (!STEADY && p <= 0) {
         // column 0 (and the lanes not started yet): no diagonal, no deletions
 #pragma unroll
@@ -338,6 +382,8 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
       lgx = long_exponent(bmx);
       lgy = long_exponent(bmy);
     }
+    lmx = lm.x;
+    lmy = lm.y;
   };
 
   // the strips, each run until both halves' bottoms are in the window
@@ -345,6 +391,11 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   for (int strip = 0; strip < nstrips && (okx || oky); ++strip) {
     const bool last = strip == nstrips - 1;
     const int ns = min(SR, n - strip * SR);
+    // the predicted boost spread evenly over the lanes holding read rows
+    const int used = (ns + R - 1) / R;
+    const int lrows = lane < used ? min(R, ns - lane * R) : 0;
+    klx = lane < used ? (lane + 1) * Bx / used - lane * Bx / used : 0;
+    kly = lane < used ? (lane + 1) * By / used - lane * By / used : 0;
     for (int attempt = 0;; ++attempt) {
       run_strip(strip, last);
       const bool gx = !okx || (lgx >= kLongFloor && lgx < kLongCeil);
@@ -355,14 +406,18 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
         if (!gy) { oky = false; fail_y = true; }
         break;
       }
-      // correct the boost of a half that left the window by what it measured
-      // (half a bit per row when it overflowed or underflowed completely)
-      auto correct = [&](int& B, int lg) {
-        const int step = (lg == 1024) ? -ns / 2 : (lg == -1024) ? ns / 2 : -lg;
-        B = max(-4 * ns, min(4 * ns, B + (step != 0 ? step : (lg > 0 ? -1 : 1))));
-      };
-      if (!gx) correct(Bx, lgx);
-      if (!gy) correct(By, lgy);
+      // a half that left the window takes each lane's measured decay
+      const int in0 = strip == 0 ? kLongStart : 0;
+      if (!gx) klx = relane(klx, lmx, used, lrows, in0, lane);
+      if (!gy) kly = relane(kly, lmy, used, lrows, in0, lane);
+    }
+    // the strip's boost per half: the sum of its lanes' shares
+    Bx = klx;
+    By = kly;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      Bx += __shfl_xor_sync(FULL, Bx, o);
+      By += __shfl_xor_sync(FULL, By, o);
     }
     // the boosts of the strip count into the exponent (plus the first strip's start)
     const int start = strip == 0 ? kLongStart : 0;
