@@ -74,6 +74,8 @@ def parse():
                     help="run vardepth_b200.autotune on a 2%% region sample first (auto: every forward workload)")
     ap.add_argument("--long-mode", choices=["warp", "block", "single"], default=None,
                     help="fix the long-read path (vd_tuning.long_mode) instead of autotuning it")
+    ap.add_argument("--long-group", type=int, default=None,
+                    help="with --long-mode: haplotypes per long-read warp item (vd_tuning.long_group, 1..8)")
     ap.add_argument("--workload", default="batched_regions",
                     choices=["batched_regions", "long_haplotype_stress", "planted_error_model", "mixed_length_regions"],
                     help="batched_regions (default) is the metric's workload; the others print their own line")
@@ -491,7 +493,8 @@ def main():
     tuned = None
     if args.long_mode is not None:
         engine.set_tuning(**dict(engine.tuning(), long_mode={"warp": native.VD_LONG_WARP, "block": native.VD_LONG_BLOCK,
-                                                             "single": native.VD_LONG_SINGLE}[args.long_mode]))
+                                                             "single": native.VD_LONG_SINGLE}[args.long_mode],
+                                 long_group=args.long_group or 0))
     elif args.autotune == "on" or args.autotune == "auto":
         from vardepth_b200 import autotune
         tlog = []

@@ -149,7 +149,13 @@ typedef struct vd_tuning {
   int pair_split;       /* two-read items with at least this many rows per lane (6, the default, or 7)
                            run on the 12-warp-per-SM kernel (168 registers), fewer rows on the
                            16-warp kernel (128 registers); 0 = 6 */
-  int reserved[2];      /* must be zero */
+  int long_group;       /* VD_LONG_WARP: haplotypes per long-read item, 1..8 (0 = 8).  The item's
+                           warp runs them two at a time; the pairs after the first take each
+                           strip's lane boosts from the first pair's measured decays (the read's
+                           errors sit at the same rows against every haplotype), so fewer strips
+                           run twice.  Fewer haplotypes per item leave more items for a batch
+                           of few long reads.  VD_LONG_BLOCK items hold two haplotypes. */
+  int reserved[1];      /* must be zero */
 } vd_tuning;
 enum { VD_LONG_WARP = 0, VD_LONG_SINGLE = 1, VD_LONG_BLOCK = 2 };
 int vd_engine_set_tuning(vd_engine *engine, const vd_tuning *tuning);

@@ -597,12 +597,13 @@ def _long_read_regions(seed, lengths, err, n_haps):
 
 @pytest.mark.parametrize("err,n_haps", [(0.08, 3), (0.01, 4)])
 def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
-    """Reads of 257, 1,500 and 10,000 bases in the long-read kernel (one read against two
-    haplotypes per warp, per-lane power-of-two boosts): within 1e-4 log10 of the FP64 oracle
-    with no pair left to FP64 and the genotype argmax unchanged, bit-identical under the plain
-    schedule (one haplotype per item).  The same bound and the same plain/batched identity hold
-    for the block-per-pair kernel (the CTA's 4 warps split each 1,024-row strip), for 128-row
-    strips and for the single-read path."""
+    """Reads of 257, 1,500 and 10,000 bases in the long-read kernel (one read against up to
+    eight haplotypes per warp item, two at a time, per-lane power-of-two boosts, the pairs
+    after the first starting from its measured lane decays): within 1e-4 log10 of the FP64
+    oracle with no pair left to FP64 and the genotype argmax unchanged, bit-identical under the
+    plain schedule.  The same bound and the same plain/batched identity hold for items of two
+    and three haplotypes, for the block-per-pair kernel (the CTA's 4 warps split each
+    1,024-row strip), for 128-row strips and for the single-read path."""
     w = _long_read_regions(int(err * 1000) + n_haps, [257, 1500, 10000], err, n_haps)
     want = _oracle_workload(w)
     eng = native.Engine(0, 8192)
@@ -614,9 +615,11 @@ def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
     assert _argmax_agree(w, got, want) == (w.n_regions, w.n_regions)
     np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], got)
     # other strip heights and the single-read path: within the bound, plain still bit-identical
-    for rows, mode in [(256, native.VD_LONG_BLOCK), (128, native.VD_LONG_BLOCK), (128, native.VD_LONG_WARP),
-                       (256, native.VD_LONG_SINGLE), (128, native.VD_LONG_SINGLE), (64, native.VD_LONG_WARP)]:
-        eng.set_tuning(long_read_rows=rows, long_mode=mode)
+    for rows, mode, group in [(256, native.VD_LONG_BLOCK, 0), (128, native.VD_LONG_BLOCK, 0),
+                              (128, native.VD_LONG_WARP, 0), (256, native.VD_LONG_WARP, 2),
+                              (256, native.VD_LONG_WARP, 3), (256, native.VD_LONG_SINGLE, 0),
+                              (128, native.VD_LONG_SINGLE, 0), (64, native.VD_LONG_WARP, 0)]:
+        eng.set_tuning(long_read_rows=rows, long_mode=mode, long_group=group)
         other = eng.forward(_packed(w), batched)[0]
         assert_mixed_close(other, want)
         np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], other)

@@ -23,7 +23,11 @@ lays out the work list:
   CTA whose warps split each strip (``VD_LONG_BLOCK``: more parallelism per
   pair, for batches of few long pairs), or one pair per warp in the
   single-read kernel with exact strip renormalisation and the drift tier
-  behind it (``VD_LONG_SINGLE``).
+  behind it (``VD_LONG_SINGLE``);
+* ``long_group``  haplotypes per warp item of a long read (8, 4, 2): the
+  pairs after an item's first start each strip from the lane boosts the first
+  pair measured, so larger items rerun fewer strips, smaller ones leave more
+  items to balance the tail of a batch of few long reads.
 
 ``autotune`` times candidate settings with resident plans (CUDA events around
 the captured tier graph) on a seeded region sample of the caller's batch,
@@ -41,8 +45,9 @@ import numpy as np
 from . import native
 
 DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0, "long_mode": native.VD_LONG_WARP,
-           "pair_split": 6}
+           "pair_split": 6, "long_group": native.LONG_GROUP_MAX}
 SPACE = {
+    "long_group": [native.LONG_GROUP_MAX, 4, 2],
     "pair_split": [6, 7],
     "long_mode": [native.VD_LONG_WARP, native.VD_LONG_BLOCK, native.VD_LONG_SINGLE],
     "long_read_rows": [256, 128, 64],
@@ -86,7 +91,7 @@ def _time(engine: native.Engine, packed: native.Packed, params, setting: dict, r
     return float(np.median(ms))
 
 
-LONG_KNOBS = ("long_mode", "long_read_rows")     # act on reads longer than one strip only
+LONG_KNOBS = ("long_mode", "long_read_rows", "long_group")     # act on reads longer than one strip only
 SHORT_KNOBS = ("pair_split", "pair_mask", "max_item_columns")
 
 

@@ -38,6 +38,7 @@ namespace vd {
 
 constexpr int kWarp = 32;
 constexpr int kMaxR = 8;                       // read rows per lane
+constexpr int kLongGroupMax = 8;               // haplotypes of one long-read warp item
 constexpr int kStripRows = kWarp * kMaxR;      // rows per strip of a long read
 constexpr int kWarpsPerBlock = 4;
 constexpr int kDriftTier = 3;  // tier number of the FP32 drift-compensated rescue (pairhmm_kernel.cuh)

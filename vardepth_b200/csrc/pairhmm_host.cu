@@ -180,13 +180,17 @@ struct vd_engine {
   size_t budget = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
+  // the long-read kernel runs on a side stream beside the other primary
+  // kernels: as its persistent blocks run out of items, theirs take the SMs
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::mutex mu;
   int grid[2][2] = {{0, 0}, {0, 0}};  // [f64][anchored] blocks
   int grid_pair[2][2] = {{0, 0}, {0, 0}};  // blocks of the two-read kernels [split == 7][wide]
   int grid_drift = 0;                 // blocks of the drift tier (no more than grid[0][0])
   int grid_long[2][2] = {{0, 0}, {0, 0}};  // blocks of the long-read kernels [block][R == 8] (<= grid[0][0])
   int grid_grad[2] = {0, 0};          // blocks of the gradient kernel [f64]
-  vd_tuning tuning{256, 0x1fe, 0, 0, VD_LONG_WARP, 6, {0, 0}};  // vd_engine_set_tuning
+  vd_tuning tuning{256, 0x1fe, 0, 0, VD_LONG_WARP, 6, kLongGroupMax, {0}};  // vd_engine_set_tuning
   DevBuf grad_arena;                  // inputs, lists and scratch of vd_forward_backward
   DevBuf geno_arena;                  // buffers of vd_region_genotypes
   // table cache
@@ -203,8 +207,9 @@ struct vd_engine {
   // so one chunk's host work-list build and upload overlap the other's kernels
   struct Slot {
     DevBuf arena;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join = nullptr;
     unsigned long long* hcnt = nullptr;  // pinned copy of the tier counters
     std::vector<double> stage;           // pair-form outputs before the scatter
     vd_plan* pl = nullptr;
@@ -302,6 +307,7 @@ struct BuildOpts {
   int long_R = kMaxR;              // rows per lane of reads longer than one 256-row strip
   bool long_warp = true;           // such reads (FP32 semiglobal) run a read against two haplotypes per item
   bool long_block = false;         // ... on a block per item (the CTA's warps split each strip)
+  int long_group = kLongGroupMax;  // haplotypes per warp item of such a read
   int pair_split = 6;              // two-read items with this many rows per lane or more: 12-warp kernel
   int pair_mask = 0x1fe;           // bit R: two reads of R rows per lane may share a warp
   int64_t max_stream = 1 << 30;    // haplotype columns one work item streams at most
@@ -322,6 +328,7 @@ BuildOpts build_opts(const vd_engine* e) {
   bo.long_warp = (e->tuning.long_mode == VD_LONG_WARP || e->tuning.long_mode == VD_LONG_BLOCK) &&
                  (bo.long_R == 8 || bo.long_R == 4);
   bo.long_block = e->tuning.long_mode == VD_LONG_BLOCK;
+  bo.long_group = bo.long_block ? 2 : e->tuning.long_group > 0 ? e->tuning.long_group : kLongGroupMax;
   bo.pair_split = e->tuning.pair_split == 7 ? 7 : 6;
   return bo;
 }
@@ -581,30 +588,37 @@ void build_region_chunk(const vd_batch* b, int64_t g0, int64_t g1, const TableSe
       region_order_and_shares(b, h_lo, h_hi, c.ha, c.hap_order.data() + (h_lo - c.ha),
                               c.hap_share.data() + (h_lo - c.ha));
     // a long read (FP32 semiglobal, one-sided emission) against its region's
-    // non-empty haplotypes, two neighbours per item (one in the plain schedule)
+    // non-empty haplotypes: runs of up to long_group neighbours per item, in
+    // both schedules (the haplotypes after an item's first pair take their
+    // boosts from it, so the grouping is part of the result)
     auto emit_long = [&](int64_t r) {
       const int32_t code = c.read_code[r - c.ra];
       const int n = (int)(c.read_off[r - c.ra + 1] - c.read_off[r - c.ra]);
       const int64_t rows = (int64_t)kWarp * bo.long_R * ((n + kWarp * bo.long_R - 1) / (kWarp * bo.long_R));
       auto len = [&](int64_t h) { return (int)(b->hap_off[h + 1] - b->hap_off[h]); };
       for (int64_t h = h_lo; h < h_hi;) {
-        const int m = len(h);
-        if (m <= 0) { ++h; continue; }
-        const bool two = !plain && h + 1 < h_hi && len(h + 1) > 0;
-        const int m2 = two ? len(h + 1) : 0;
+        if (len(h) <= 0) { ++h; continue; }
+        int k = 1;
+        while (k < bo.long_group && h + k < h_hi && len(h + k) > 0) ++k;
+        int64_t work = 0, cells = 0;
+        for (int j = 0; j < k; j += 2) {
+          const int ma = len(h + j), mb = j + 1 < k ? len(h + j + 1) : 0;
+          work += rows * (std::max(ma, mb) + 1 + kWarp) * (j + 1 < k ? 2 : 1);
+          cells += (int64_t)n * (ma + mb);
+        }
         WorkItem w;
         w.read = (int32_t)(r - c.ra);
-        w.nhap = two ? 2 : 1;
+        w.nhap = k;
         w.hap_begin = h - c.ha;
         w.out_begin = region_out + (r - r_lo) * nh + (h - h_lo);
         w.code = (code & ~15) | bo.long_R | kLongBit;
         w.read2 = -1;
         w.out2_begin = 0;
         items.push_back(w);
-        cost.push_back(rows * (std::max(m, m2) + 1 + kWarp) * (two ? 2 : 1));
-        sl.cells += (int64_t)n * (m + m2);
-        sl.pairs += two ? 2 : 1;
-        h += two ? 2 : 1;
+        cost.push_back(work);
+        sl.cells += cells;
+        sl.pairs += k;
+        h += k;
       }
     };
     // emit the haplotype runs of read r (and r2 >= 0 riding along)
@@ -887,6 +901,8 @@ struct vd_plan {
   // or a pipeline slot's in vd_forward)
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_mid = nullptr, ev_end = nullptr;
+  cudaStream_t side = nullptr;                        // the long-read kernel's stream
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // its fork from and join into `stream`
   int64_t last_rescued1 = 0, last_rescued2 = 0;
 };
 
@@ -984,8 +1000,28 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   if (!pl->chunk.items.empty()) {
     cudaError_t err = cudaSuccess;
     const int64_t np = pl->chunk.n_paired, nw = pl->chunk.n_paired_wide;
-    // two-read items first, on their own kernels (FP32 semiglobal only):
-    // 6-8 rows per lane, then up to 5
+    const int64_t nl = pl->chunk.n_long;
+    q.static_order = pl->params.schedule == VD_SCHEDULE_PLAIN ? 1 : 0;
+    if (nl > 0) {
+      // long reads, up to kLongGroupMax haplotypes per warp item, launched
+      // first on the side stream: the kernels below take the SMs its blocks
+      // leave as its queue runs dry, so they fill its tail; its failures join
+      // the spill list
+      VD_CUDA(cudaEventRecord(pl->ev_fork, pl->stream));
+      VD_CUDA(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
+      QueueView ql = q;
+      ql.items = (const WorkItem*)(d + L.o_items) + np;
+      ql.n_items = nl;
+      ql.head = cnt + 10;
+      const int R = pl->chunk.long_R;
+      const bool blk = pl->chunk.long_block;
+      err = launch_long_f32(R, blk, bv, ql, &dt->f32, ht->s32d, e->grid_long[blk ? 1 : 0][R == 8 ? 1 : 0], pl->side);
+      if (err != cudaSuccess) return cuda_fail(err, "long-read tier launch");
+      ++n;
+      VD_CUDA(cudaEventRecord(pl->ev_join, pl->side));
+    }
+    // two-read items, on their own kernels (FP32 semiglobal only): 6-8 rows
+    // per lane, then up to 5
     for (int k = 0; k < 2; ++k) {
       const int64_t lo = k ? nw : 0, hi = k ? np : nw;
       if (hi <= lo) continue;
@@ -999,20 +1035,6 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       if (err != cudaSuccess) return cuda_fail(err, "two-read tier launch");
       ++n;
     }
-    q.static_order = pl->params.schedule == VD_SCHEDULE_PLAIN ? 1 : 0;
-    const int64_t nl = pl->chunk.n_long;
-    if (nl > 0) {
-      // long reads, two haplotypes per warp; their failures join the spill list
-      QueueView ql = q;
-      ql.items = (const WorkItem*)(d + L.o_items) + np;
-      ql.n_items = nl;
-      ql.head = cnt + 10;
-      const int R = pl->chunk.long_R;
-      const bool blk = pl->chunk.long_block;
-      err = launch_long_f32(R, blk, bv, ql, &dt->f32, ht->s32d, e->grid_long[blk ? 1 : 0][R == 8 ? 1 : 0], pl->stream);
-      if (err != cudaSuccess) return cuda_fail(err, "long-read tier launch");
-      ++n;
-    }
     q.items = (const WorkItem*)(d + L.o_items) + np + nl;
     q.n_items = (long long)(pl->chunk.items.size() - np - nl);
     if (q.n_items > 0) {
@@ -1021,6 +1043,7 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       if (err != cudaSuccess) return cuda_fail(err, "primary tier launch");
       ++n;
     }
+    if (nl > 0) VD_CUDA(cudaStreamWaitEvent(pl->stream, pl->ev_join, 0));
     VD_CUDA(cudaEventRecordWithFlags(pl->ev_mid, pl->stream, evflags));
     BatchView rv = bv;
     rv.hap_sel = nullptr;
@@ -1239,6 +1262,9 @@ int vd_engine_create(int device, int64_t memory_mb, vd_engine** out) {
   if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_begin)) != cudaSuccess || (err = cudaEventCreate(&e->ev_mid)) != cudaSuccess ||
       (err = cudaEventCreate(&e->ev_end)) != cudaSuccess ||
+      (err = cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (err = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (err = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming)) != cudaSuccess ||
       (err = cudaMallocHost((void**)&e->htab, sizeof(TableSet))) != cudaSuccess) {
     rc = cuda_fail(err, "engine setup");
   }
@@ -1247,6 +1273,9 @@ int vd_engine_create(int device, int64_t memory_mb, vd_engine** out) {
     if ((err = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (err = cudaEventCreate(&sl.ev[0])) != cudaSuccess || (err = cudaEventCreate(&sl.ev[1])) != cudaSuccess ||
         (err = cudaEventCreate(&sl.ev[2])) != cudaSuccess ||
+        (err = cudaStreamCreateWithFlags(&sl.side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (err = cudaEventCreateWithFlags(&sl.fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (err = cudaEventCreateWithFlags(&sl.join, cudaEventDisableTiming)) != cudaSuccess ||
         (err = cudaMallocHost((void**)&sl.hcnt, 16 * sizeof(unsigned long long))) != cudaSuccess)
       rc = cuda_fail(err, "engine pipeline setup");
   }
@@ -1261,6 +1290,7 @@ int vd_engine_destroy(vd_engine* e) {
   {
     DeviceGuard guard(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->side) cudaStreamSynchronize(e->side);
     // plans still alive become empty shells; vd_plan_destroy frees the shell
     for (vd_plan* pl : e->plans) {
       if (pl->graph) cudaGraphExecDestroy(pl->graph);
@@ -1272,11 +1302,15 @@ int vd_engine_destroy(vd_engine* e) {
     e->plans.clear();
     for (vd_engine::Slot& sl : e->slots) {
       if (sl.stream) cudaStreamSynchronize(sl.stream);
+      if (sl.side) cudaStreamSynchronize(sl.side);
       delete sl.pl;
       sl.pl = nullptr;
       sl.arena.release();
       for (cudaEvent_t& ev : sl.ev) if (ev) cudaEventDestroy(ev);
+      if (sl.fork) cudaEventDestroy(sl.fork);
+      if (sl.join) cudaEventDestroy(sl.join);
       if (sl.hcnt) cudaFreeHost(sl.hcnt);
+      if (sl.side) cudaStreamDestroy(sl.side);
       if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     e->arena.release();
@@ -1287,6 +1321,9 @@ int vd_engine_destroy(vd_engine* e) {
     if (e->ev_begin) cudaEventDestroy(e->ev_begin);
     if (e->ev_mid) cudaEventDestroy(e->ev_mid);
     if (e->ev_end) cudaEventDestroy(e->ev_end);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_join) cudaEventDestroy(e->ev_join);
+    if (e->side) cudaStreamDestroy(e->side);
     if (e->stream) cudaStreamDestroy(e->stream);
   }
   if (e == g_default) g_default = nullptr;
@@ -1314,7 +1351,9 @@ int vd_engine_set_tuning(vd_engine* e, const vd_tuning* t) {
     return fail(VD_EINVAL, "long_mode must be VD_LONG_WARP, VD_LONG_SINGLE or VD_LONG_BLOCK");
   if (t->pair_split != 0 && t->pair_split != 6 && t->pair_split != 7)
     return fail(VD_EINVAL, "pair_split must be 6 or 7 (0 = 6)");
-  for (int i = 0; i < 2; ++i) if (t->reserved[i]) return fail(VD_EINVAL, "reserved fields must be zero");
+  if (t->long_group < 0 || t->long_group > kLongGroupMax)
+    return fail(VD_EINVAL, "long_group must be 1..8 (0 = 8)");
+  if (t->reserved[0]) return fail(VD_EINVAL, "reserved fields must be zero");
   std::lock_guard<std::mutex> lk(e->mu);
   e->tuning = *t;
   return VD_OK;
@@ -1453,6 +1492,9 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     pl.ev_begin = sl.ev[0];
     pl.ev_mid = sl.ev[1];
     pl.ev_end = sl.ev[2];
+    pl.side = sl.side;
+    pl.ev_fork = sl.fork;
+    pl.ev_join = sl.join;
     const double th = now_ms();
     const bool plain = p->schedule == VD_SCHEDULE_PLAIN;
     const BuildOpts bo = build_opts(e);
@@ -1514,6 +1556,9 @@ int vd_plan_create(vd_engine* e, const vd_batch* b, const vd_params* p, vd_plan*
   pl->ev_begin = e->ev_begin;
   pl->ev_mid = e->ev_mid;
   pl->ev_end = e->ev_end;
+  pl->side = e->side;
+  pl->ev_fork = e->ev_fork;
+  pl->ev_join = e->ev_join;
   if (p->quality_offsets) {
     pl->has_offsets = true;
     for (int i = 0; i < 4; ++i) pl->offsets[i] = p->quality_offsets[i];

@@ -146,16 +146,28 @@ __device__ __forceinline__ int relane(const int kl, const float lm, const int us
   return max(-96, min(120, k));
 }
 
-// One work item: read w.read against haplotypes hap_begin and hap_begin + 1
-// (nhap = 2) or hap_begin alone (nhap = 1); outputs out_begin (+1).
+// Strips of a read whose per-lane decays the first pair of an item records
+// (longer reads predict the rest from the mean rate), and the window a lane's
+// bottom-row maximum must end in for a run to be kept.
+constexpr int kLongProfStrips = 80;
+// Boost bits per row a strip may take (an error-rich read at 8% errors and
+// reported Q30 takes about one; a random read against a random haplotype
+// four to five)
+constexpr int kLongMaxRate = 4;
+constexpr int kLongLaneFloor = -90;
+constexpr int kLongLaneCeil = 90;
+
+// One work item: read w.read against haplotypes hap_begin .. hap_begin +
+// nhap - 1 (nhap <= kLongGroupMax), two at a time; outputs out_begin + k.
 // `scratch` is the warp's slot: 2 * half float4 boundary records (half >= the
 // longest haplotype + 1); `ring` and `oring` 32 float4 each of shared memory
-// per warp (the boundary read, the boundary written).
+// per warp (the boundary read, the boundary written); `prof` the warp's
+// kLongProfStrips x 32 per-lane decays.
 template <int R>
 __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv, const WorkItem w,
                                           const Tables<float>* __restrict__ tb, const Scalars<float> sc,
                                           const int lane, float4* __restrict__ scratch, float4* __restrict__ ring,
-                                          float4* __restrict__ oring) {
+                                          float4* __restrict__ oring, short* __restrict__ prof) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr double kLn2 = 0.6931471805599453094;
   constexpr int SR = kWarp * R;
@@ -163,13 +175,12 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   const int n = (int)(bv.read_off[w.read + 1] - roff);
   const uint8_t* __restrict__ rbase = bv.read_bases + roff;
   const uint8_t* __restrict__ rqual = bv.read_quals + roff;
-  const bool two = w.nhap > 1;
-  const int64_t h1 = w.hap_begin, h2 = two ? w.hap_begin + 1 : w.hap_begin;
-  const int64_t ho1 = bv.hap_off[h1], ho2 = bv.hap_off[h2];
-  const int m1 = (int)(bv.hap_off[h1 + 1] - ho1), m2 = (int)(bv.hap_off[h2 + 1] - ho2);
-  const uint8_t* __restrict__ hp1 = bv.hap_bases + ho1 - 1;  // hp[j] = base of column j >= 1
-  const uint8_t* __restrict__ hp2 = bv.hap_bases + ho2 - 1;
-  const int M = max(m1, m2);
+  // the pair in hand (set for each pair of the item)
+  bool two = false;
+  int64_t h1 = 0, h2 = 0;
+  int m1 = 0, m2 = 0, M = 0;
+  const uint8_t* __restrict__ hp1 = nullptr;  // hp[j] = base of column j >= 1
+  const uint8_t* __restrict__ hp2 = nullptr;
   const int nstrips = (n + SR - 1) / SR;
   const long long half = qv.scratch_stride / 2;
 
@@ -182,6 +193,7 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   const float c0 = sc.c;
 
   // per half: boost bits of the current strip, total exponent, still in play
+  // (reset for each pair)
   int Bx = 0, By = 0, Ex = 0, Ey = 0;
   // decay measured over the strips done so far (bits, rows): the next strip's
   // boost is this mean rate times its rows.  A single strip's decay scatters
@@ -386,84 +398,141 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
     lmy = lm.y;
   };
 
-  // the strips, each run until both halves' bottoms are in the window
-  bool fail_x = false, fail_y = !two;
-  for (int strip = 0; strip < nstrips && (okx || oky); ++strip) {
-    const bool last = strip == nstrips - 1;
-    const int ns = min(SR, n - strip * SR);
-    // the predicted boost spread evenly over the lanes holding read rows
-    const int used = (ns + R - 1) / R;
-    const int lrows = lane < used ? min(R, ns - lane * R) : 0;
-    klx = lane < used ? (lane + 1) * Bx / used - lane * Bx / used : 0;
-    kly = lane < used ? (lane + 1) * By / used - lane * By / used : 0;
-    for (int attempt = 0;; ++attempt) {
-      run_strip(strip, last);
-      const bool gx = !okx || (lgx >= kLongFloor && lgx < kLongCeil);
-      const bool gy = !oky || (lgy >= kLongFloor && lgy < kLongCeil);
-      if (gx && gy) break;
-      if (attempt + 1 == kLongTries) {
-        if (!gx) { okx = false; fail_x = true; }
-        if (!gy) { oky = false; fail_y = true; }
-        break;
-      }
-      // a half that left the window takes each lane's measured decay
-      const int in0 = strip == 0 ? kLongStart : 0;
-      if (!gx) klx = relane(klx, lmx, used, lrows, in0, lane);
-      if (!gy) kly = relane(kly, lmy, used, lrows, in0, lane);
-    }
-    // the strip's boost per half: the sum of its lanes' shares
-    Bx = klx;
-    By = kly;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-      Bx += __shfl_xor_sync(FULL, Bx, o);
-      By += __shfl_xor_sync(FULL, By, o);
-    }
-    // the boosts of the strip count into the exponent (plus the first strip's start)
-    const int start = strip == 0 ? kLongStart : 0;
-    if (!last) {
-      // the next strip reads this one's boundary brought to 2^0 (|lg| <= 60, so
-      // one exact factor); its boost is this strip's decay, scaled to its rows
-      const int ksx = okx ? -lgx : 0, ksy = oky ? -lgy : 0;
-      inx = ksx;
-      iny = ksy;
-      const int ns1 = min(SR, n - (strip + 1) * SR);
-      Nrows += ns;
-      if (okx) {
-        Ex += Bx + start + ksx;
-        Dx += Bx + start - lgx;
-        Bx = max(0, min(4 * ns1, Dx * ns1 / Nrows));
-      }
-      if (oky) {
-        Ey += By + start + ksy;
-        Dy += By + start - lgy;
-        By = max(0, min(4 * ns1, Dy * ns1 / Nrows));
-      }
-    } else {
-      Ex += Bx + start;
-      Ey += By + start;
-    }
-  }
+  // the item's first pair records each strip's per-lane decays (of its first
+  // half while that is in play, else its second); the pairs after it start a
+  // recorded strip from them and the rest from the mean rate
+  int prof_len = 0;
+  // every lane holding read rows ended its bottom row in the lane window
+  auto lanes_in_window = [&](const float lm, const int used) -> bool {
+    const int lg = long_exponent(lm);
+    return __all_sync(FULL, lane >= used || (lg >= kLongLaneFloor && lg < kLongLaneCeil));
+  };
 
-  if (lane == kWarp - 1) {
-    const double lnC1 = sc.ln_c + log((double)(m1 + 1));
-    const double lnC2 = sc.ln_c + log((double)(m2 + 1));
-    if (okx && !fail_x) {
-      bv.out[w.out_begin] = log(zx) - lnC1 + lnN - (double)Ex * kLn2;
-    } else {
-      bv.out[w.out_begin] = __longlong_as_double(0x7ff8000000000000LL);
-      spill_pair<float>(qv, w.read, h1, w.out_begin);
-    }
-    if (two) {
-      if (oky && !fail_y) {
-        bv.out[w.out_begin + 1] = log(zy) - lnC2 + lnN - (double)Ey * kLn2;
+  for (int g = 0; g < w.nhap; g += 2) {
+    two = g + 1 < w.nhap;
+    h1 = w.hap_begin + g;
+    h2 = two ? h1 + 1 : h1;
+    const int64_t ho1 = bv.hap_off[h1], ho2 = bv.hap_off[h2];
+    m1 = (int)(bv.hap_off[h1 + 1] - ho1);
+    m2 = (int)(bv.hap_off[h2 + 1] - ho2);
+    hp1 = bv.hap_bases + ho1 - 1;
+    hp2 = bv.hap_bases + ho2 - 1;
+    M = max(m1, m2);
+    Bx = By = Ex = Ey = 0;
+    Dx = Dy = Nrows = 0;
+    int Gx = 0, Gy = 0;  // boost bits taken so far, per half
+    okx = true;
+    oky = two;
+    inx = iny = 0;
+    lgx = lgy = 0;
+    zx = zy = 0.0;
+
+    // the strips, each run until both halves' bottoms are in the window
+    bool fail_x = false, fail_y = !two;
+    for (int strip = 0; strip < nstrips && (okx || oky); ++strip) {
+      const bool last = strip == nstrips - 1;
+      const int ns = min(SR, n - strip * SR);
+      const int used = (ns + R - 1) / R;  // lanes holding read rows
+      const int lrows = lane < used ? min(R, ns - lane * R) : 0;
+      const int in0 = strip == 0 ? kLongStart : 0;  // exponent of the strip's input
+      if (g > 0 && strip < prof_len) {
+        // the first pair's decay of each lane, aiming its bottom at 2^0
+        const int d = lane < used ? (int)prof[strip * kWarp + lane] : 0;
+        klx = lane < used ? max(-96, min(120, d - (lane == 0 ? in0 : 0))) : 0;
+        kly = klx;
       } else {
-        bv.out[w.out_begin + 1] = __longlong_as_double(0x7ff8000000000000LL);
-        spill_pair<float>(qv, w.read, h2, w.out_begin + 1);
+        // the predicted boost spread evenly over the lanes holding read rows
+        klx = lane < used ? (lane + 1) * Bx / used - lane * Bx / used : 0;
+        kly = lane < used ? (lane + 1) * By / used - lane * By / used : 0;
+      }
+      for (int attempt = 0;; ++attempt) {
+        run_strip(strip, last);
+        const bool gx = !okx || (lgx >= kLongFloor && lgx < kLongCeil && lanes_in_window(lmx, used));
+        const bool gy = !oky || (lgy >= kLongFloor && lgy < kLongCeil && lanes_in_window(lmy, used));
+        if (gx && gy) break;
+        if (attempt + 1 == kLongTries) {
+          if (!gx) { okx = false; fail_x = true; }
+          if (!gy) { oky = false; fail_y = true; }
+          break;
+        }
+        // a half that left the window takes each lane's measured decay
+        if (!gx) klx = relane(klx, lmx, used, lrows, in0, lane);
+        if (!gy) kly = relane(kly, lmy, used, lrows, in0, lane);
+      }
+      // the strip's boost per half: the sum of its lanes' shares
+      Bx = klx;
+      By = kly;
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        Bx += __shfl_xor_sync(FULL, Bx, o);
+        By += __shfl_xor_sync(FULL, By, o);
+      }
+      // a half that needed more than kLongMaxRate bits per row over the read so
+      // far (and 64 bits of slack) is beyond what this tier keeps exact
+      // (alignment families that trade places across rows sit far below the
+      // row maximum): it goes to the drift and FP64 tiers
+      Gx += Bx;
+      Gy += By;
+      if (okx && Gx > kLongMaxRate * (Nrows + ns) + 64) { okx = false; fail_x = true; }
+      if (oky && Gy > kLongMaxRate * (Nrows + ns) + 64) { oky = false; fail_y = true; }
+      if (g == 0 && strip == prof_len && strip < kLongProfStrips && (okx || oky)) {
+        const int lg = long_exponent(okx ? lmx : lmy);
+        int in = __shfl_up_sync(FULL, lg, 1);
+        if (lane == 0) in = in0;
+        prof[strip * kWarp + lane] = (short)(lane < used ? (okx ? klx : kly) + in - lg : 0);
+        ++prof_len;
+      }
+      // the boosts of the strip count into the exponent (plus the first strip's start)
+      if (!last) {
+        // the next strip reads this one's boundary brought to 2^0 (|lg| <= 60, so
+        // one exact factor); its boost is the read's mean decay rate so far
+        // times its rows
+        const int ksx = okx ? -lgx : 0, ksy = oky ? -lgy : 0;
+        inx = ksx;
+        iny = ksy;
+        const int ns1 = min(SR, n - (strip + 1) * SR);
+        Nrows += ns;
+        if (okx) {
+          Ex += Bx + in0 + ksx;
+          Dx += Bx + in0 - lgx;
+          Bx = max(0, min(4 * ns1, Dx * ns1 / Nrows));
+        }
+        if (oky) {
+          Ey += By + in0 + ksy;
+          Dy += By + in0 - lgy;
+          By = max(0, min(4 * ns1, Dy * ns1 / Nrows));
+        }
+      } else {
+        Ex += Bx + in0;
+        Ey += By + in0;
       }
     }
+
+    // ln of the final sum z = f 2^e (f in [1/2, 1)) less the boosts: the bits
+    // do not depend on which powers of two the boosts took
+    if (lane == kWarp - 1) {
+      const int64_t o1 = w.out_begin + g;
+      if (okx && !fail_x) {
+        int e;
+        const double f = frexp(zx, &e);
+        bv.out[o1] = log(f) - (sc.ln_c + log((double)(m1 + 1))) + lnN + (double)(e - Ex) * kLn2;
+      } else {
+        bv.out[o1] = __longlong_as_double(0x7ff8000000000000LL);
+        spill_pair<float>(qv, w.read, h1, o1);
+      }
+      if (two) {
+        if (oky && !fail_y) {
+          int e;
+          const double f = frexp(zy, &e);
+          bv.out[o1 + 1] = log(f) - (sc.ln_c + log((double)(m2 + 1))) + lnN + (double)(e - Ey) * kLn2;
+        } else {
+          bv.out[o1 + 1] = __longlong_as_double(0x7ff8000000000000LL);
+          spill_pair<float>(qv, w.read, h2, o1 + 1);
+        }
+      }
+    }
+    __syncwarp();
   }
-  __syncwarp();
 }
 
 // Persistent kernel of the long-read items (FP32 semiglobal primary tier):
@@ -476,6 +545,7 @@ pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
                     const Scalars<float> sc) {
   __shared__ Tables<float> tab;
   __shared__ float4 rings[kWarpsPerBlock][2][kWarp];
+  __shared__ short profs[kWarpsPerBlock][kLongProfStrips * kWarp];
   {
     const int words = (int)(sizeof(Tables<float>) / sizeof(int));
     const int* src = reinterpret_cast<const int*>(gtab);
@@ -499,7 +569,7 @@ pairhmm_long_kernel(const BatchView bv, const QueueView qv, const Tables<float>*
     }
     if ((long long)i >= qv.n_items) break;
     process_long<R>(bv, qv, qv.items[i], &tab, sc, lane, scratch, rings[threadIdx.x >> 5][0],
-                    rings[threadIdx.x >> 5][1]);
+                    rings[threadIdx.x >> 5][1], profs[threadIdx.x >> 5]);
   }
 }
 

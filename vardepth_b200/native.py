@@ -21,6 +21,7 @@ VD_PRECISION_MIXED, VD_PRECISION_FLOAT64 = 0, 1
 VD_SCHEDULE_BATCHED, VD_SCHEDULE_PLAIN = 0, 1
 VD_CHECKPOINT_SQRT, VD_CHECKPOINT_ALL = 0, 1
 VD_LONG_WARP, VD_LONG_SINGLE, VD_LONG_BLOCK = 0, 1, 2
+LONG_GROUP_MAX = 8  # haplotypes of one long-read warp item (kLongGroupMax)
 
 c_i64 = ctypes.c_int64
 c_i32 = ctypes.c_int32
@@ -57,12 +58,13 @@ class VdStats(ctypes.Structure):
 class VdTuning(ctypes.Structure):
     _fields_ = [("long_read_rows", ctypes.c_int), ("pair_mask", ctypes.c_int), ("max_item_columns", ctypes.c_int),
                 ("pipeline_gcells", ctypes.c_int), ("long_mode", ctypes.c_int), ("pair_split", ctypes.c_int),
-                ("reserved", ctypes.c_int * 2)]
+                ("long_group", ctypes.c_int), ("reserved", ctypes.c_int * 1)]
 
     def as_dict(self) -> dict:
         return {"long_read_rows": self.long_read_rows, "pair_mask": self.pair_mask,
                 "max_item_columns": self.max_item_columns, "pipeline_gcells": self.pipeline_gcells,
-                "long_mode": self.long_mode, "pair_split": self.pair_split or 6}
+                "long_mode": self.long_mode, "pair_split": self.pair_split or 6,
+                "long_group": self.long_group or LONG_GROUP_MAX}
 
 
 class VdGenotypeOptions(ctypes.Structure):
@@ -320,12 +322,14 @@ class Engine:
         return t.as_dict()
 
     def set_tuning(self, long_read_rows: int = 256, pair_mask: int = 0x1FE, max_item_columns: int = 0,
-                   pipeline_gcells: int = 0, long_mode: int = VD_LONG_WARP, pair_split: int = 6) -> None:
+                   pipeline_gcells: int = 0, long_mode: int = VD_LONG_WARP, pair_split: int = 6,
+                   long_group: int = 0) -> None:
         t = VdTuning()
         t.long_read_rows, t.pair_mask, t.max_item_columns = int(long_read_rows), int(pair_mask), int(max_item_columns)
         t.pipeline_gcells = int(pipeline_gcells)
         t.long_mode = int(long_mode)
         t.pair_split = int(pair_split)
+        t.long_group = int(long_group)
         check(library().vd_engine_set_tuning(self.handle, ctypes.byref(t)), "vd_engine_set_tuning")
 
     def forward(self, packed: Packed, params: VdParams, out: np.ndarray | None = None):
