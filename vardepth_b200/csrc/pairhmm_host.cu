@@ -1430,10 +1430,33 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
   };
   int64_t total_cells = 0;
   for (int64_t u = 0; u < units; ++u) total_cells += unit_cells(u);
+  // warp items of the long-read kernel (reads longer than a strip, up to
+  // long_group haplotypes each)
+  const BuildOpts lbo = build_opts(e);
+  int64_t long_items = 0;
+  if (lbo.long_warp && !lbo.long_block && p->precision != VD_PRECISION_FLOAT64 && !p->anchored) {
+    auto long_reads = [&](int64_t r0, int64_t r1) {
+      int64_t k = 0;
+      for (int64_t r = r0; r < r1; ++r) k += (b->read_off[r + 1] - b->read_off[r]) > kStripRows;
+      return k;
+    };
+    for (int64_t u = 0; u < units; ++u) {
+      const int64_t nh = pair_form ? pg.start[u + 1] - pg.start[u] : b->region_hap_off[u + 1] - b->region_hap_off[u];
+      const int64_t nl = pair_form ? long_reads(u, u + 1) : long_reads(b->region_read_off[u], b->region_read_off[u + 1]);
+      long_items += nl * ((nh + lbo.long_group - 1) / lbo.long_group);
+    }
+  }
   // The first chunk is a quarter of the others: its host work and upload are
-  // the only ones not hidden behind kernels.
+  // the only ones not hidden behind kernels.  Chunks run one after another on
+  // the device, so each keeps at least kLongItemsPerWarp long-read items per
+  // warp (a chunk's last long items would otherwise run alone on the GPU).
+  constexpr int64_t kLongItemsPerWarp = 8;
   const int64_t pipeline_cells = (int64_t)(e->tuning.pipeline_gcells > 0 ? e->tuning.pipeline_gcells : 300) * 1'000'000'000LL;
-  const int64_t n_pipe = std::max<int64_t>(1, std::min<int64_t>(8, total_cells / pipeline_cells));
+  int64_t n_pipe = std::max<int64_t>(1, std::min<int64_t>(8, total_cells / pipeline_cells));
+  if (long_items > 0) {
+    const int64_t long_warps = (int64_t)e->grid_long[0][lbo.long_R == 8 ? 1 : 0] * kWarpsPerBlock;
+    n_pipe = std::max<int64_t>(1, std::min<int64_t>(n_pipe, long_items / (kLongItemsPerWarp * std::max<int64_t>(1, long_warps))));
+  }
   const int64_t chunk_cells = n_pipe > 1 ? (total_cells + n_pipe - 1) / n_pipe : INT64_MAX;
 
   int64_t fixed = pair_form ? (b->hap_off[b->n_haps] - b->hap_off[0]) + 8 * b->n_haps : 0;
