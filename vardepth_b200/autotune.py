@@ -24,10 +24,15 @@ lays out the work list:
   pair, for batches of few long pairs), or one pair per warp in the
   single-read kernel with exact strip renormalisation and the drift tier
   behind it (``VD_LONG_SINGLE``);
-* ``long_group``  haplotypes per warp item of a long read (8, 4, 2): the
-  pairs after an item's first start each strip from the lane boosts the first
-  pair measured, so larger items rerun fewer strips, smaller ones leave more
-  items to balance the tail of a batch of few long reads.
+* ``long_group``  haplotypes per warp item of a long read: the pairs after
+  an item's first start each strip from the lane boosts the first pair
+  measured, so larger items rerun fewer strips, smaller ones leave more items
+  to balance the tail of a batch of few long reads.  It is not searched: the
+  tail it trades against depends on how many long items the whole batch
+  holds, which a sample does not show (on the mixed-length workload a 2%
+  sample preferred 4 haplotypes per item, the 20,000-region batch runs 5%
+  faster with 8).  The default (8) stays; a batch of few long reads is better
+  served by the block or single-read path, which the search does cover.
 
 ``autotune`` times candidate settings with resident plans (CUDA events around
 the captured tier graph) on a seeded region sample of the caller's batch,
@@ -47,7 +52,6 @@ from . import native
 DEFAULT = {"long_read_rows": 256, "pair_mask": 0x1FE, "max_item_columns": 0, "long_mode": native.VD_LONG_WARP,
            "pair_split": 6, "long_group": native.LONG_GROUP_MAX}
 SPACE = {
-    "long_group": [native.LONG_GROUP_MAX, 4, 2],
     "pair_split": [6, 7],
     "long_mode": [native.VD_LONG_WARP, native.VD_LONG_BLOCK, native.VD_LONG_SINGLE],
     "long_read_rows": [256, 128, 64],
@@ -91,7 +95,7 @@ def _time(engine: native.Engine, packed: native.Packed, params, setting: dict, r
     return float(np.median(ms))
 
 
-LONG_KNOBS = ("long_mode", "long_read_rows", "long_group")     # act on reads longer than one strip only
+LONG_KNOBS = ("long_mode", "long_read_rows")     # act on reads longer than one strip only
 SHORT_KNOBS = ("pair_split", "pair_mask", "max_item_columns")
 
 
