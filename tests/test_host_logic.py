@@ -297,10 +297,15 @@ def test_autotune_samples_split_long_and_short_regions():
     w = S.mixed_length_regions(n_regions=300, workers=1)
     pk = native.Packed(w.read_bases, w.read_quals, w.read_off, w.hap_bases, w.hap_off,
                        region_read_off=w.region_read_off, region_hap_off=w.region_hap_off)
-    short, long_ = autotune.split_samples(pk, fraction=0.1, min_regions=10, long_items=50)
+    short, long_ = autotune.split_samples(pk, fraction=0.1, min_regions=10, long_items=50, short_items=1)
     longest = lambda p: [int(np.diff(p.read_off)[p.region_read_off[g]:p.region_read_off[g + 1]].max(initial=0))
                          for g in range(len(p.region_read_off) - 1)]
     assert max(longest(short)) <= 256 and min(longest(long_)) > 256
     n_long = sum(1 for v in longest(pk) if v > 256)
     assert 1 <= len(long_.region_read_off) - 1 <= n_long
     assert len(short.region_read_off) - 1 == max(10, round(0.1 * (len(w.region_read_off) - 1 - n_long)))
+    # the short sample grows to hold the requested two-read items (half its reads, rounded up per region)
+    big, _ = autotune.split_samples(pk, fraction=0.1, min_regions=10, long_items=50, short_items=2000)
+    rr = big.region_read_off
+    items = sum(int(rr[g + 1] - rr[g]) // 2 + 1 for g in range(len(rr) - 1))
+    assert items >= 2000 or len(rr) - 1 == len(w.region_read_off) - 1 - n_long

@@ -100,13 +100,16 @@ SHORT_KNOBS = ("pair_split", "pair_mask", "max_item_columns")
 
 
 def split_samples(packed: native.Packed, fraction: float = 0.02, min_regions: int = 200, long_items: int = 8192,
-                  seed: int = 2024):
+                  seed: int = 2024, short_items: int = 49152):
     """Two seeded region samples of a region-form batch: regions holding a read longer than one
     256-row strip ("long") and the others ("short").  The short sample is `fraction` of the short
-    regions (at least `min_regions`); the long sample takes long regions until it holds about
-    `long_items` read x haplotype-pair items, enough to fill every warp of the device several
-    times over, because the long kernels' time on a few long items is their slowest item's, not
-    their throughput.  Either may be None."""
+    regions (at least `min_regions`), grown until it holds about `short_items` two-read items
+    (half its reads); the long sample takes long regions until it holds about `long_items`
+    read x haplotype-pair items.  Both fill every warp of the device many times over, because a
+    persistent kernel's time on a few items per warp is its slowest warp's, not its throughput
+    (on 200 of 10,000 batched regions, about 2.5 items per warp, the single-read kernel looked
+    25% faster than the two-read kernels that run the whole batch 35% faster).  Either may be
+    None."""
     from . import shard
     rr, hh = packed.region_read_off, packed.region_hap_off
     rl = np.diff(packed.read_off)
@@ -118,8 +121,10 @@ def split_samples(packed: native.Packed, fraction: float = 0.02, min_regions: in
     out = []
     short = np.flatnonzero(~is_long)
     if len(short):
-        k = min(len(short), max(min_regions, int(round(fraction * len(short)))))
-        out.append(np.sort(rng.choice(short, size=k, replace=False)))
+        order = rng.permutation(short)
+        items = np.cumsum(np.diff(rr)[order] // 2 + 1)
+        k = max(min_regions, int(round(fraction * len(short))), int(np.searchsorted(items, short_items)) + 1)
+        out.append(np.sort(order[:min(len(short), k)]))
     else:
         out.append(None)
     long_ = np.flatnonzero(is_long)
