@@ -567,12 +567,14 @@ def main():
     torch.cuda.synchronize()
     kernel_ms = primary_ms = 0.0
     rescued = drift_rescued = launches = shared = 0
+    long_strips = long_runs = 0
     for _ in range(args.steps):
         st = plan.run()
         kernel_ms += st.kernel_ms
         primary_ms += st.primary_ms
         rescued = st.rescued_fp64 + st.rescued_robust
         drift_rescued = st.rescued_fp32
+        long_strips, long_runs = st.long_strips, st.long_strip_runs
         shared = st.shared_cells
         launches += st.kernel_launches
     torch.cuda.synchronize()
@@ -785,6 +787,10 @@ def main():
             "rescued_pairs": int(rescued), "rescued_fraction": round(rescued / max(1, mine.n_outputs()), 6),
             "rescued_fp32_drift_pairs": int(drift_rescued), "parity": parity, "clocks": sampler.summary(),
         }
+        if long_strips:
+            # the long-read warp kernel: strips (per pair of an item) and their runs
+            line["long_read_strips"] = {"strips": int(long_strips), "runs": int(long_runs),
+                                        "runs_per_strip": round(long_runs / long_strips, 4)}
         print(json.dumps(line), flush=True)
     engine.close()
     if dist is not None:

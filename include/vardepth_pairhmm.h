@@ -109,6 +109,8 @@ typedef struct vd_stats {
                                haplotype of the region and were not streamed again */
   int64_t rescued_fp32;     /* pairs the primary tier spilled that the FP32 drift tier (per-row
                                power-of-two boosts, semiglobal) resolved */
+  int64_t long_strips;      /* strips of the long-read warp kernel (per pair of an item) */
+  int64_t long_strip_runs;  /* their runs: a strip whose bottom left the window runs again */
 } vd_stats;
 
 typedef struct vd_engine vd_engine;

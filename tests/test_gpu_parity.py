@@ -612,6 +612,11 @@ def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
     got, st = eng.forward(_packed(w), batched)
     assert_mixed_close(got, want)
     assert st.rescued_fp64 + st.rescued_robust == 0 and st.rescued_fp32 == 0
+    # every pair of haplotypes (two per pair, up to 8 per item) runs the read's strips at least once
+    n_strips = sum(-(-int(n) // 256) * -(-int(w.region_hap_off[g + 1] - w.region_hap_off[g]) // 2)
+                   for g in range(w.n_regions)
+                   for n in np.diff(w.read_off)[w.region_read_off[g]:w.region_read_off[g + 1]])
+    assert st.long_strips == n_strips and st.long_strip_runs >= st.long_strips
     assert _argmax_agree(w, got, want) == (w.n_regions, w.n_regions)
     np.testing.assert_array_equal(eng.forward(_packed(w), plain)[0], got)
     # other strip heights and the single-read path: within the bound, plain still bit-identical

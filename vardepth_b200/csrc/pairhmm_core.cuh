@@ -125,6 +125,7 @@ struct QueueView {
   long long scratch_stride;   // in boundary records (float2 / double2)
   int* error_flag;            // set when the spill list overflows
   int static_order;           // 1: warp w takes items w, w + W, w + 2W ... (W = warps in the grid)
+  unsigned long long* strip_runs;  // long-read kernel, nullable: [0] runs of strips, [1] strips
 };
 
 }  // namespace vd

@@ -974,8 +974,8 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
   cudaGetLastError();  // launch checks below must see only their own errors
   // cnt[0..2] work heads of tiers 0..2, cnt[3], cnt[4] spill counts, cnt[5] error flag,
   // cnt[6..7] heads of the two-read kernels, cnt[8] spill count of the FP64
-  // tier, cnt[9] head of the drift tier (FP32 semiglobal only) and cnt[10]
-  // head of the long-read kernel
+  // tier, cnt[9] head of the drift tier (FP32 semiglobal only), cnt[10]
+  // head of the long-read kernel, cnt[11..12] its runs of strips and strips
   VD_CUDA(cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), pl->stream));
   VD_CUDA(cudaEventRecordWithFlags(pl->ev_begin, pl->stream, evflags));
   const BatchView bv = batch_view(pl);
@@ -1013,6 +1013,7 @@ int enqueue_tiers(vd_plan* pl, int* launches, bool capturing = false) {
       ql.items = (const WorkItem*)(d + L.o_items) + np;
       ql.n_items = nl;
       ql.head = cnt + 10;
+      ql.strip_runs = cnt + 11;  // cnt[11] runs of strips, cnt[12] strips
       const int R = pl->chunk.long_R;
       const bool blk = pl->chunk.long_block;
       err = launch_long_f32(R, blk, bv, ql, &dt->f32, ht->s32d, e->grid_long[blk ? 1 : 0][R == 8 ? 1 : 0], pl->side);
@@ -1114,15 +1115,18 @@ int tier_times(const vd_plan* pl, double* total, double* primary, double* rescue
 }
 
 int enqueue_counter_read(vd_plan* pl, unsigned long long* host) {
-  VD_CUDA(cudaMemcpyAsync(host, pl->base + pl->L.o_cnt, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+  VD_CUDA(cudaMemcpyAsync(host, pl->base + pl->L.o_cnt, 13 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                           pl->stream));
   return VD_OK;
 }
 
 // after the plan's stream completed: pairs rescued by the drift tier (r0),
 // recomputed in the FP64 wavefront (r1) and in FP64 32-row strips (r2)
-int check_counters(const vd_plan* pl, const unsigned long long* h, int64_t* r0, int64_t* r1, int64_t* r2) {
+int check_counters(const vd_plan* pl, const unsigned long long* h, int64_t* r0, int64_t* r1, int64_t* r2,
+                   int64_t* runs = nullptr, int64_t* strips = nullptr) {
   if (h[5]) return fail(VD_EOVERFLOW, "rescue list overflow");
+  if (runs) *runs = (int64_t)h[11];
+  if (strips) *strips = (int64_t)h[12];
   const bool f64 = pl->params.precision == VD_PRECISION_FLOAT64;
   const bool drift = !f64 && !pl->params.anchored;
   *r0 = drift ? (int64_t)(h[3] - h[4]) : 0;
@@ -1131,12 +1135,12 @@ int check_counters(const vd_plan* pl, const unsigned long long* h, int64_t* r0, 
   return VD_OK;
 }
 
-int read_counters(vd_plan* pl, int64_t* r0, int64_t* r1, int64_t* r2) {
-  unsigned long long h[9];
+int read_counters(vd_plan* pl, int64_t* r0, int64_t* r1, int64_t* r2, int64_t* runs, int64_t* strips) {
+  unsigned long long h[13];
   int rc = enqueue_counter_read(pl, h);
   if (rc) return rc;
   VD_CUDA(cudaStreamSynchronize(pl->stream));
-  return check_counters(pl, h, r0, r1, r2);
+  return check_counters(pl, h, r0, r1, r2, runs, strips);
 }
 
 int init_engine_grids(vd_engine* e) {
@@ -1474,10 +1478,12 @@ int vd_forward(vd_engine* e, const vd_batch* b, const vd_params* p, double* out,
     sl.busy = false;
     VD_CUDA(cudaStreamSynchronize(sl.stream));
     vd_plan& pl = *sl.pl;
-    int64_t r0 = 0, r1 = 0, r2 = 0;
-    int r = check_counters(&pl, sl.hcnt, &r0, &r1, &r2);
+    int64_t r0 = 0, r1 = 0, r2 = 0, lr = 0, ls = 0;
+    int r = check_counters(&pl, sl.hcnt, &r0, &r1, &r2, &lr, &ls);
     if (r) return r;
     if ((r = tier_times(&pl, &s.kernel_ms, &s.primary_ms, &s.rescue_ms))) return r;
+    s.long_strip_runs += lr;
+    s.long_strips += ls;
     s.rescued_fp32 += r0;
     s.rescued_fp64 += r1;
     s.rescued_robust += r2;
@@ -1635,8 +1641,8 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
     launches = pl->graph_launches;
   }
   VD_CUDA(cudaGraphLaunch(pl->graph, e->stream));
-  int64_t r0 = 0, r1 = 0, r2 = 0;
-  if ((rc = read_counters(pl, &r0, &r1, &r2))) return rc;
+  int64_t r0 = 0, r1 = 0, r2 = 0, lr = 0, ls = 0;
+  if ((rc = read_counters(pl, &r0, &r1, &r2, &lr, &ls))) return rc;
   double ms = 0.0, pms = 0.0, rms = 0.0;
   if ((rc = tier_times(pl, &ms, &pms, &rms))) return rc;
   pl->last_rescued1 = r1;
@@ -1651,6 +1657,8 @@ int vd_plan_run(vd_plan* pl, vd_stats* st) {
     s.rescued_fp32 = r0;
     s.rescued_fp64 = r1;
     s.rescued_robust = r2;
+    s.long_strip_runs = lr;
+    s.long_strips = ls;
     s.kernel_launches = launches;
     s.kernel_ms = ms;
     s.primary_ms = pms;

@@ -447,6 +447,10 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
       }
       for (int attempt = 0;; ++attempt) {
         run_strip(strip, last);
+        if (qv.strip_runs != nullptr && lane == 0) {
+          atomicAdd(qv.strip_runs, 1ull);
+          if (attempt == 0) atomicAdd(qv.strip_runs + 1, 1ull);
+        }
         const bool gx = !okx || (lgx >= kLongFloor && lgx < kLongCeil && lanes_in_window(lmx, used));
         const bool gy = !oky || (lgy >= kLongFloor && lgy < kLongCeil && lanes_in_window(lmy, used));
         if (gx && gy) break;

@@ -49,7 +49,8 @@ class VdStats(ctypes.Structure):
                 ("rescued_fp64", c_i64), ("rescued_robust", c_i64), ("h2d_bytes", c_i64), ("d2h_bytes", c_i64),
                 ("kernel_launches", c_i64), ("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("host_ms", ctypes.c_double), ("live_bytes", c_i64), ("primary_ms", ctypes.c_double),
-                ("rescue_ms", ctypes.c_double), ("shared_cells", c_i64), ("rescued_fp32", c_i64)]
+                ("rescue_ms", ctypes.c_double), ("shared_cells", c_i64), ("rescued_fp32", c_i64),
+                ("long_strips", c_i64), ("long_strip_runs", c_i64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
