@@ -175,12 +175,6 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   const int n = (int)(bv.read_off[w.read + 1] - roff);
   const uint8_t* __restrict__ rbase = bv.read_bases + roff;
   const uint8_t* __restrict__ rqual = bv.read_quals + roff;
-  // the pair in hand (set for each pair of the item)
-  bool two = false;
-  int64_t h1 = 0, h2 = 0;
-  int m1 = 0, m2 = 0, M = 0;
-  const uint8_t* __restrict__ hp1 = nullptr;  // hp[j] = base of column j >= 1
-  const uint8_t* __restrict__ hp2 = nullptr;
   const int nstrips = (n + SR - 1) / SR;
   const long long half = qv.scratch_stride / 2;
 
@@ -191,212 +185,6 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   const float A = tb->A[rqual[n - 1]];
   const float2 k2 = make_float2(sc.k2, sc.k2), x = make_float2(sc.x, sc.x);
   const float c0 = sc.c;
-
-  // per half: boost bits of the current strip, total exponent, still in play
-  // (reset for each pair)
-  int Bx = 0, By = 0, Ex = 0, Ey = 0;
-  // decay measured over the strips done so far (bits, rows): the next strip's
-  // boost is this mean rate times its rows.  A single strip's decay scatters
-  // by tens of bits around the read's rate (the number of errors in 256 rows),
-  // so the mean predicts the next strip about sqrt(2) times better than the
-  // last strip alone, and fewer strips run twice
-  int Dx = 0, Dy = 0, Nrows = 0;
-  bool okx = true, oky = two;
-  int inx = 0, iny = 0;        // shifts that bring the boundary above to 2^0, per half
-  int lgx = 0, lgy = 0;        // bottom exponents of the last run
-  double zx = 0.0, zy = 0.0;   // final sums (last strip, lane 31)
-  int klx = 0, kly = 0;        // this lane's share of the strip's boost, per half
-  float lmx = 0.f, lmy = 0.f;  // this lane's bottom-row maxima in the last run
-
-  // One run of strip `strip` with Bx / By boost bits; reads boundary buffer
-  // src_half, writes the other.  Sets lgx / lgy (bottom maximum or final sum).
-  auto run_strip = [&](const int strip, const bool last) {
-    const int i0 = strip * SR;
-    const int ns = min(SR, n - i0);           // read rows of the strip
-    const int lanes_used = (ns + R - 1) / R;  // lanes holding read rows
-    LongRows<R> rw;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = i0 + lane * R + r;
-      if (i < n) {
-        const unsigned q = rqual[i];
-        rw.rb[r] = rbase[i];
-        rw.miss[r] = tb->miss[q];
-        const float K = tb->K[q], X = (i == n - 1) ? A : tb->X[q];
-        rw.K[r] = make_float2(K, K);
-        rw.X[r] = make_float2(X, X);
-      } else {  // past the read: pass u down the column
-        rw.rb[r] = kNeverBase;
-        rw.miss[r] = 0.f;
-        rw.K[r] = make_float2(0.f, 0.f);
-        rw.X[r] = make_float2(1.f, 1.f);
-      }
-      rw.W[r] = make_float2(0.f, 0.f);
-      rw.s[r] = make_float2(0.f, 0.f);
-    }
-    // lane L's share of the boost: floor((L+1) B / lanes) - floor(L B / lanes)
-    // over the lanes holding read rows; the first strip's input starts at 2^kLongStart
-    // (|B| <= 4 ns keeps every share within +-4R, far inside the float exponent range)
-    boost_row0(rw, make_float2(pow2T(klx, 0.f), pow2T(kly, 0.f)));
-    const float cin = c0 * pow2T(kLongStart, 0.f);  // the first strip's row-0 value
-    float4* const src = scratch + (long long)(strip & 1) * half;
-    float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
-    // the boundary above is stored as written (its maximum at 2^lg); it is
-    // brought to 2^0 as it is loaded, by 2^-lg per half
-    const float fsx = pow2T(inx, 0.f), fsy = pow2T(iny, 0.f);
-
-    float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
-    double accx = 0.0, accy = 0.0;
-    float bmx = 0.f, bmy = 0.f;
-    float2 lm = make_float2(0.f, 0.f);  // this lane's bottom-row maxima
-    const bool lane0 = lane == 0;
-    // boundary records of the strip above, staged through the warp's ring:
-    // every 32 steps each lane loads one record of the next 32 columns, and
-    // at every step all lanes read the record of lane 0's column (a broadcast)
-    float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
-    auto load_window = [&](int base) -> float4 {
-      const int p = base + lane;
-      if (strip == 0 || p > M) return make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 v = src[p];
-      return make_float4(v.x * fsx, v.y * fsx, v.z * fsy, v.w * fsy);
-    };
-    auto stage_window = [&](int t) {
-      __syncwarp();
-      ring[lane] = nxt;
-      __syncwarp();
-      nxt = load_window(t + kWarp);
-    };
-    // this strip's bottom rows: lane 31 lays each column's record into the
-    // warp's out-ring, and every 32 columns the warp writes them to the
-    // boundary buffer in one coalesced store and folds them into the maxima
-    int flushed = 0;  // columns below this are in the boundary buffer
-    auto flush_out = [&](int count) {
-      __syncwarp();
-      if (lane < count) {
-        const int p = flushed + lane;
-        const float4 rec = oring[lane];
-        dst[p] = rec;
-        if (p <= m1) bmx = fmaxf(bmx, fmaxf(rec.x, rec.y));
-        if (p <= m2) bmy = fmaxf(bmy, fmaxf(rec.z, rec.w));
-      }
-      __syncwarp();
-      flushed += count;
-    };
-    // lane 31 moves its FP32 row sums into FP64 after its columns 8r+7
-    auto flush_acc = [&]() {
-      accx += (double)acc32.x;
-      accy += (double)acc32.y;
-      acc32 = make_float2(0.f, 0.f);
-    };
-    const float2 cin2 = make_float2(cin, cin);
-    // one step; STEADY: every lane inside both haplotypes at a column >= 1
-    auto step = [&](auto steady_tag, const int t) {
-      constexpr bool STEADY = decltype(steady_tag)::value;
-      const int p = t - lane;  // this lane's column
-      float2 u_in = shfl_up2(u_bot);
-      float2 s_in = shfl_up2(rw.s[R - 1]);
-      float2 in_s = cin2, in_u = cin2;
-      if (strip > 0) {
-        const float4 rec = ring[t & (kWarp - 1)];
-        in_s = make_float2(rec.x, rec.z);
-        in_u = make_float2(rec.y, rec.w);
-      }
-      u_in = lane0 ? in_u : u_in;
-      s_in = lane0 ? in_s : s_in;
-      bool inside = true;
-      uint32_t hbx, hby;
-      if (STEADY) {
-        hbx = hp1[p];
-        hby = hp2[p];
-      } else {
-        // column 0 has no base (kNeverBase never matches); past a haplotype's
-        // end its half reads that haplotype's last base (its columns are not used)
-        inside = p >= 0 && p <= M;
-        hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
-        hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
-      }
-      column_long<R>(rw, hbx, hby, (STEADY || p > 0) ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
-      if (STEADY) {
-        lm.x = fmaxf(lm.x, u_bot.x);
-        lm.y = fmaxf(lm.y, u_bot.y);
-      } else {
-        if (inside && p <= m1) lm.x = fmaxf(lm.x, u_bot.x);
-        if (inside && p <= m2) lm.y = fmaxf(lm.y, u_bot.y);
-      }
-      if (!STEADY && p <= 0) {
-        // column 0 (and the lanes not started yet): no diagonal, no deletions
-#pragma unroll
-        for (int r = 0; r < R; ++r) rw.W[r] = make_float2(0.f, 0.f);
-      }
-      s_top = s_in;
-      if (last) {
-        // the final row sums (lane 31's are the ones used)
-        if (STEADY) {
-          acc32 = __fadd2_rn(acc32, u_bot);
-        } else if (lane == kWarp - 1 && inside) {
-          if (p <= m1) acc32.x += u_bot.x;
-          if (p <= m2) acc32.y += u_bot.y;
-          if ((p & 7) == 7) flush_acc();
-        }
-      } else if (lane == kWarp - 1 && inside) {
-        oring[p & (kWarp - 1)] = make_float4(rw.s[R - 1].x, u_bot.x, rw.s[R - 1].y, u_bot.y);
-      }
-    };
-    // the out-ring is full when lane 31 has finished column flushed + 31
-    auto maybe_flush = [&](int t) {
-      if (!last && t - (kWarp - 1) == flushed + kWarp - 1) flush_out(kWarp);
-    };
-
-    nxt = load_window(0);
-    const int steps = M + 1 + (kWarp - 1);
-    // steady steps: every lane at a column in 1 .. min(m1, m2)
-    const int t_lo = kWarp, t_hi = min(m1, m2) + 1;
-    int t = 0;
-    for (; t < steps && (t < t_lo || (t < t_hi && (t & 7) != 0)); ++t) {
-      if ((t & (kWarp - 1)) == 0) stage_window(t);
-      step(std::false_type{}, t);
-      maybe_flush(t);
-    }
-    // blocks of 8 steps start at a multiple of 8, so lane 31's columns 8r+7
-    // fall at the block's step 6 and its out-ring fills at step 6 of every
-    // fourth block
-    for (; t + 8 <= t_hi; t += 8) {
-      if ((t & (kWarp - 1)) == 0) stage_window(t);
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        step(std::true_type{}, t + u);
-        if (u == 6) {
-          if (last) flush_acc();
-          else maybe_flush(t + u);
-        }
-      }
-    }
-    for (; t < steps; ++t) {
-      if ((t & (kWarp - 1)) == 0) stage_window(t);
-      step(std::false_type{}, t);
-      maybe_flush(t);
-    }
-    if (!last && flushed <= M) flush_out(M + 1 - flushed);
-    if (!last) {
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        bmx = fmaxf(bmx, __shfl_xor_sync(FULL, bmx, o));
-        bmy = fmaxf(bmy, __shfl_xor_sync(FULL, bmy, o));
-      }
-    }
-    __syncwarp();
-    if (last) {
-      zx = __shfl_sync(FULL, accx + (double)acc32.x, kWarp - 1);
-      zy = __shfl_sync(FULL, accy + (double)acc32.y, kWarp - 1);
-      lgx = long_exponent(zx);
-      lgy = long_exponent(zy);
-    } else {
-      lgx = long_exponent(bmx);
-      lgy = long_exponent(bmy);
-    }
-    lmx = lm.x;
-    lmy = lm.y;
-  };
 
   // the item's first pair records each strip's per-lane decays (of its first
   // half while that is in play, else its second); the pairs after it start a
@@ -409,23 +197,220 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
   };
 
   for (int g = 0; g < w.nhap; g += 2) {
-    two = g + 1 < w.nhap;
-    h1 = w.hap_begin + g;
-    h2 = two ? h1 + 1 : h1;
+    // the pair in hand
+    const bool two = g + 1 < w.nhap;
+    const int64_t h1 = w.hap_begin + g, h2 = two ? h1 + 1 : h1;
     const int64_t ho1 = bv.hap_off[h1], ho2 = bv.hap_off[h2];
-    m1 = (int)(bv.hap_off[h1 + 1] - ho1);
-    m2 = (int)(bv.hap_off[h2 + 1] - ho2);
-    hp1 = bv.hap_bases + ho1 - 1;
-    hp2 = bv.hap_bases + ho2 - 1;
-    M = max(m1, m2);
-    Bx = By = Ex = Ey = 0;
-    Dx = Dy = Nrows = 0;
-    int Gx = 0, Gy = 0;  // boost bits taken so far, per half
-    okx = true;
-    oky = two;
-    inx = iny = 0;
-    lgx = lgy = 0;
-    zx = zy = 0.0;
+    const int m1 = (int)(bv.hap_off[h1 + 1] - ho1), m2 = (int)(bv.hap_off[h2 + 1] - ho2);
+    const uint8_t* __restrict__ hp1 = bv.hap_bases + ho1 - 1;  // hp[j] = base of column j >= 1
+    const uint8_t* __restrict__ hp2 = bv.hap_bases + ho2 - 1;
+    const int M = max(m1, m2);
+
+    // per half: boost bits of the current strip, total exponent, still in play
+    int Bx = 0, By = 0, Ex = 0, Ey = 0;
+    // decay measured over the strips done so far (bits, rows): the next strip's
+    // boost is this mean rate times its rows.  A single strip's decay scatters
+    // by tens of bits around the read's rate (the number of errors in 256 rows),
+    // so the mean predicts the next strip about sqrt(2) times better than the
+    // last strip alone, and fewer strips run twice
+    int Dx = 0, Dy = 0, Nrows = 0;
+    bool okx = true, oky = two;
+    int inx = 0, iny = 0;        // shifts that bring the boundary above to 2^0, per half
+    int lgx = 0, lgy = 0;        // bottom exponents of the last run
+    double zx = 0.0, zy = 0.0;   // final sums (last strip, lane 31)
+    int klx = 0, kly = 0;        // this lane's share of the strip's boost, per half
+    float lmx = 0.f, lmy = 0.f;  // this lane's bottom-row maxima in the last run
+
+    // One run of strip `strip` with Bx / By boost bits; reads boundary buffer
+    // src_half, writes the other.  Sets lgx / lgy (bottom maximum or final sum).
+    auto run_strip = [&](const int strip, const bool last) {
+      const int i0 = strip * SR;
+      const int ns = min(SR, n - i0);           // read rows of the strip
+      const int lanes_used = (ns + R - 1) / R;  // lanes holding read rows
+      LongRows<R> rw;
+  #pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = i0 + lane * R + r;
+        if (i < n) {
+          const unsigned q = rqual[i];
+          rw.rb[r] = rbase[i];
+          rw.miss[r] = tb->miss[q];
+          const float K = tb->K[q], X = (i == n - 1) ? A : tb->X[q];
+          rw.K[r] = make_float2(K, K);
+          rw.X[r] = make_float2(X, X);
+        } else {  // past the read: pass u down the column
+          rw.rb[r] = kNeverBase;
+          rw.miss[r] = 0.f;
+          rw.K[r] = make_float2(0.f, 0.f);
+          rw.X[r] = make_float2(1.f, 1.f);
+        }
+        rw.W[r] = make_float2(0.f, 0.f);
+        rw.s[r] = make_float2(0.f, 0.f);
+      }
+      // lane L's share of the boost: floor((L+1) B / lanes) - floor(L B / lanes)
+      // over the lanes holding read rows; the first strip's input starts at 2^kLongStart
+      // (|B| <= 4 ns keeps every share within +-4R, far inside the float exponent range)
+      boost_row0(rw, make_float2(pow2T(klx, 0.f), pow2T(kly, 0.f)));
+      const float cin = c0 * pow2T(kLongStart, 0.f);  // the first strip's row-0 value
+      float4* const src = scratch + (long long)(strip & 1) * half;
+      float4* const dst = scratch + (long long)((strip + 1) & 1) * half;
+      // the boundary above is stored as written (its maximum at 2^lg); it is
+      // brought to 2^0 as it is loaded, by 2^-lg per half
+      const float fsx = pow2T(inx, 0.f), fsy = pow2T(iny, 0.f);
+
+      float2 s_top = make_float2(0.f, 0.f), u_bot = make_float2(0.f, 0.f), acc32 = make_float2(0.f, 0.f);
+      double accx = 0.0, accy = 0.0;
+      float bmx = 0.f, bmy = 0.f;
+      float2 lm = make_float2(0.f, 0.f);  // this lane's bottom-row maxima
+      const bool lane0 = lane == 0;
+      // boundary records of the strip above, staged through the warp's ring:
+      // every 32 steps each lane loads one record of the next 32 columns, and
+      // at every step all lanes read the record of lane 0's column (a broadcast)
+      float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+      auto load_window = [&](int base) -> float4 {
+        const int p = base + lane;
+        if (strip == 0 || p > M) return make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 v = src[p];
+        return make_float4(v.x * fsx, v.y * fsx, v.z * fsy, v.w * fsy);
+      };
+      auto stage_window = [&](int t) {
+        __syncwarp();
+        ring[lane] = nxt;
+        __syncwarp();
+        nxt = load_window(t + kWarp);
+      };
+      // this strip's bottom rows: lane 31 lays each column's record into the
+      // warp's out-ring, and every 32 columns the warp writes them to the
+      // boundary buffer in one coalesced store and folds them into the maxima
+      int flushed = 0;  // columns below this are in the boundary buffer
+      auto flush_out = [&](int count) {
+        __syncwarp();
+        if (lane < count) {
+          const int p = flushed + lane;
+          const float4 rec = oring[lane];
+          dst[p] = rec;
+          if (p <= m1) bmx = fmaxf(bmx, fmaxf(rec.x, rec.y));
+          if (p <= m2) bmy = fmaxf(bmy, fmaxf(rec.z, rec.w));
+        }
+        __syncwarp();
+        flushed += count;
+      };
+      // lane 31 moves its FP32 row sums into FP64 after its columns 8r+7
+      auto flush_acc = [&]() {
+        accx += (double)acc32.x;
+        accy += (double)acc32.y;
+        acc32 = make_float2(0.f, 0.f);
+      };
+      const float2 cin2 = make_float2(cin, cin);
+      // one step; STEADY: every lane inside both haplotypes at a column >= 1
+      auto step = [&](auto steady_tag, const int t) {
+        constexpr bool STEADY = decltype(steady_tag)::value;
+        const int p = t - lane;  // this lane's column
+        float2 u_in = shfl_up2(u_bot);
+        float2 s_in = shfl_up2(rw.s[R - 1]);
+        float2 in_s = cin2, in_u = cin2;
+        if (strip > 0) {
+          const float4 rec = ring[t & (kWarp - 1)];
+          in_s = make_float2(rec.x, rec.z);
+          in_u = make_float2(rec.y, rec.w);
+        }
+        u_in = lane0 ? in_u : u_in;
+        s_in = lane0 ? in_s : s_in;
+        bool inside = true;
+        uint32_t hbx, hby;
+        if (STEADY) {
+          hbx = hp1[p];
+          hby = hp2[p];
+        } else {
+          // column 0 has no base (kNeverBase never matches); past a haplotype's
+          // end its half reads that haplotype's last base (its columns are not used)
+          inside = p >= 0 && p <= M;
+          hbx = (inside && p > 0) ? (uint32_t)hp1[min(p, m1)] : kNeverBase;
+          hby = (inside && p > 0) ? (uint32_t)hp2[min(p, m2)] : kNeverBase;
+        }
+        column_long<R>(rw, hbx, hby, (STEADY || p > 0) ? s_top : make_float2(0.f, 0.f), u_in, k2, x, u_bot);
+        if (STEADY) {
+          lm.x = fmaxf(lm.x, u_bot.x);
+          lm.y = fmaxf(lm.y, u_bot.y);
+        } else {
+          if (inside && p <= m1) lm.x = fmaxf(lm.x, u_bot.x);
+          if (inside && p <= m2) lm.y = fmaxf(lm.y, u_bot.y);
+        }
+        if (!STEADY && p <= 0) {
+          // column 0 (and the lanes not started yet): no diagonal, no deletions
+  #pragma unroll
+          for (int r = 0; r < R; ++r) rw.W[r] = make_float2(0.f, 0.f);
+        }
+        s_top = s_in;
+        if (last) {
+          // the final row sums (lane 31's are the ones used)
+          if (STEADY) {
+            acc32 = __fadd2_rn(acc32, u_bot);
+          } else if (lane == kWarp - 1 && inside) {
+            if (p <= m1) acc32.x += u_bot.x;
+            if (p <= m2) acc32.y += u_bot.y;
+            if ((p & 7) == 7) flush_acc();
+          }
+        } else if (lane == kWarp - 1 && inside) {
+          oring[p & (kWarp - 1)] = make_float4(rw.s[R - 1].x, u_bot.x, rw.s[R - 1].y, u_bot.y);
+        }
+      };
+      // the out-ring is full when lane 31 has finished column flushed + 31
+      auto maybe_flush = [&](int t) {
+        if (!last && t - (kWarp - 1) == flushed + kWarp - 1) flush_out(kWarp);
+      };
+
+      nxt = load_window(0);
+      const int steps = M + 1 + (kWarp - 1);
+      // steady steps: every lane at a column in 1 .. min(m1, m2)
+      const int t_lo = kWarp, t_hi = min(m1, m2) + 1;
+      int t = 0;
+      for (; t < steps && (t < t_lo || (t < t_hi && (t & 7) != 0)); ++t) {
+        if ((t & (kWarp - 1)) == 0) stage_window(t);
+        step(std::false_type{}, t);
+        maybe_flush(t);
+      }
+      // blocks of 8 steps start at a multiple of 8, so lane 31's columns 8r+7
+      // fall at the block's step 6 and its out-ring fills at step 6 of every
+      // fourth block
+      for (; t + 8 <= t_hi; t += 8) {
+        if ((t & (kWarp - 1)) == 0) stage_window(t);
+  #pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          step(std::true_type{}, t + u);
+          if (u == 6) {
+            if (last) flush_acc();
+            else maybe_flush(t + u);
+          }
+        }
+      }
+      for (; t < steps; ++t) {
+        if ((t & (kWarp - 1)) == 0) stage_window(t);
+        step(std::false_type{}, t);
+        maybe_flush(t);
+      }
+      if (!last && flushed <= M) flush_out(M + 1 - flushed);
+      if (!last) {
+  #pragma unroll
+        for (int o = 16; o; o >>= 1) {
+          bmx = fmaxf(bmx, __shfl_xor_sync(FULL, bmx, o));
+          bmy = fmaxf(bmy, __shfl_xor_sync(FULL, bmy, o));
+        }
+      }
+      __syncwarp();
+      if (last) {
+        zx = __shfl_sync(FULL, accx + (double)acc32.x, kWarp - 1);
+        zy = __shfl_sync(FULL, accy + (double)acc32.y, kWarp - 1);
+        lgx = long_exponent(zx);
+        lgy = long_exponent(zy);
+      } else {
+        lgx = long_exponent(bmx);
+        lgy = long_exponent(bmy);
+      }
+      lmx = lm.x;
+      lmy = lm.y;
+    };
+
 
     // the strips, each run until both halves' bottoms are in the window
     bool fail_x = false, fail_y = !two;
@@ -471,14 +456,13 @@ __device__ __noinline__ void process_long(const BatchView bv, const QueueView qv
         Bx += __shfl_xor_sync(FULL, Bx, o);
         By += __shfl_xor_sync(FULL, By, o);
       }
-      // a half that needed more than kLongMaxRate bits per row over the read so
-      // far (and 64 bits of slack) is beyond what this tier keeps exact
-      // (alignment families that trade places across rows sit far below the
-      // row maximum): it goes to the drift and FP64 tiers
-      Gx += Bx;
-      Gy += By;
-      if (okx && Gx > kLongMaxRate * (Nrows + ns) + 64) { okx = false; fail_x = true; }
-      if (oky && Gy > kLongMaxRate * (Nrows + ns) + 64) { oky = false; fail_y = true; }
+      // a half whose read decayed by more than kLongMaxRate bits per row so far
+      // (with 64 bits of slack and the first strip's 2^60 start) is beyond what
+      // this tier keeps exact (alignment families that trade places across
+      // rows sit far below the row maximum): it goes to the drift and FP64 tiers
+      const int cap = kLongMaxRate * (Nrows + ns) + 64 + kLongStart;
+      if (okx && Dx + Bx + in0 - lgx > cap) { okx = false; fail_x = true; }
+      if (oky && Dy + By + in0 - lgy > cap) { oky = false; fail_y = true; }
       if (g == 0 && strip == prof_len && strip < kLongProfStrips && (okx || oky)) {
         const int lg = long_exponent(okx ? lmx : lmy);
         int in = __shfl_up_sync(FULL, lg, 1);
