@@ -290,6 +290,35 @@ def test_pipelined_chunks_agree():
     eng.close()
 
 
+def test_pipeline_chunks_with_long_reads_and_long_group():
+    """vd_forward on a batch with reads longer than a strip: asking for many pipeline chunks gives
+    one here (each chunk keeps at least 8 long-read items per warp, and 300 regions hold far
+    fewer), with the single-chunk results bit for bit.  long_group takes 1..8 (0 = 8); another
+    grouping of a long read's haplotypes moves its likelihoods within FP32 rounding only."""
+    w = S.mixed_length_regions(n_regions=300, workers=1)
+    assert (np.diff(w.read_off) > 256).any()
+    eng = native.Engine(0, 8192)
+    params, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    eng.set_tuning(pipeline_gcells=1_000_000)
+    one, st1 = eng.forward(_packed(w), params)
+    assert st1.batches == 1 and st1.long_strips > 0
+    eng.set_tuning(pipeline_gcells=1)
+    many, stn = eng.forward(_packed(w), params)
+    assert stn.batches == 1
+    np.testing.assert_array_equal(many, one)
+    for bad in (-1, 9):
+        with pytest.raises(ValueError):
+            eng.set_tuning(long_group=bad)
+    eng.set_tuning(long_group=1)
+    assert eng.tuning()["long_group"] == 1
+    single, st = eng.forward(_packed(w), params)
+    assert st.long_strip_runs >= st.long_strips > st1.long_strips
+    finite = np.isfinite(one)
+    assert np.array_equal(finite, np.isfinite(single))
+    np.testing.assert_allclose(single[finite], one[finite], rtol=0, atol=1e-4)
+    eng.close()
+
+
 def test_plan_graph_replay_is_deterministic():
     w = S.batched_regions(n_regions=16)
     eng = native.Engine(0, 4096)
