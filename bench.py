@@ -621,8 +621,9 @@ def main():
         plain = {"value": round(plain_value, 3), "unit": "GCUPS", "ms_per_step": round(plain_ms, 3),
                  "steps": plain_steps, "gpu_launches": plain_launches,
                  "batched_over_plain": round(value / plain_value, 3),
-                 "schedule": "VD_SCHEDULE_PLAIN: one pair per warp item, fixed 8 rows per lane, "
-                             "input order, static round-robin over a fixed grid; same tiers and "
+                 "schedule": "VD_SCHEDULE_PLAIN: one pair per warp item (a read longer than a strip: "
+                             "the batched schedule's items of up to long_group haplotypes), fixed 8 rows "
+                             "per lane, input order, static round-robin over a fixed grid; same tiers and "
                              "arithmetic, results bit-identical to the batched schedule"}
 
     # ---- end to end through vd_forward with pinned host buffers (e2e) ----
