@@ -1,38 +1,40 @@
 // Long reads (more rows than one 256-row strip), FP32, semiglobal: one warp
-// runs one read against TWO haplotypes of its region at once.
+// runs one read against up to kLongGroupMax haplotypes of its region, TWO at
+// a time.
 //
-// The read's rows are packed as float2 over the two haplotypes (x: the first,
-// y: the second), so every FMA serves both pairs (fma.rn.f32x2) and the read's
-// per-row constants, its strip count and its strip bookkeeping are shared: the
-// pairs of one warp always have the same number of strips, which two reads of
-// different lengths would not.  A region's haplotypes differ by a few small
-// edits, so their lengths nearly agree and the shorter one idles for a few
-// columns at most.
+// The read's rows are packed as float2 over the two haplotypes of a pair (x:
+// the first, y: the second), so every FMA serves both (fma.rn.f32x2) and the
+// read's per-row constants, its strip count and its strip bookkeeping are
+// shared: the halves always have the same number of strips, which two reads
+// of different lengths would not.  A region's haplotypes differ by a few
+// small edits, so their lengths nearly agree and the shorter one idles for a
+// few columns at most.
 //
 // Range.  An error-rich read (8% errors at reported Q30) loses about one bit
 // per row along its best path, far more over a 256-row strip than FP32 holds,
-// so each strip is given B boost bits: lane L multiplies the two values it
-// receives from the lane above (or the strip boundary) by 2^k_L, k_L being
-// lane L's share of B.  A boost on a lane's inputs scales the lane's rows and
-// everything below by an exact power of two, so the rows keep the one-sided
-// emission (a match costs no multiply) and the boosts are undone exactly in
-// the final exponent.  B is measured as the read goes: each strip's decay is
-// read off the exponent of its boundary maximum, strip s+1 takes the read's
-// mean decay rate so far times its rows, and a strip whose bottom leaves
-// 2^-60 .. 2^60 is run again with B corrected by what it measured (its input
-// boundary is kept: the warp's slot holds two boundary buffers, one read and
-// one written).  The first strip has nothing to learn from, so its input
-// starts at 2^60: one pass takes any decay up to 120 bits; an error-rich
-// read's first strip (about 240) runs again with a corrected rate.  A
-// strip's boundary is stored as computed and brought to 2^0 by an exact power
-// of two as the next strip loads it.  A pair still out of range after kLongTries runs of a strip goes to the drift
-// and FP64 tiers.
+// so lane L scales everything it takes from above by 2^k_L.  A boost on a
+// lane's inputs scales the lane's rows and everything below by an exact power
+// of two, so the rows keep the one-sided emission (a match costs no multiply)
+// and the boosts are undone exactly in the final exponent.  The first pair of
+// an item spreads each strip's predicted decay (the read's mean rate so far
+// times the strip's rows) evenly over the lanes; a strip whose bottom leaves
+// 2^-60 .. 2^60, or a lane whose bottom-row maximum leaves 2^-90 .. 2^90, is
+// run again with each lane's measured decay (its input boundary is kept: the
+// warp's slot holds two boundary buffers, one read and one written).  The
+// pairs after the first start each strip from the first pair's measured lane
+// decays, since the read's errors sit at the same rows against every
+// haplotype.  The first strip starts from 2^60.  A strip's boundary is stored
+// as computed and brought to 2^0 by an exact power of two as the next strip
+// loads it.  A pair still out of range after kLongTries runs of a strip, or
+// decaying faster than kLongMaxRate bits per row, goes to the drift and FP64
+// tiers.
 //
-// Every choice above depends on the pair's own data only (B, the re-runs of a
-// strip and its renormalisation are per half; a re-run caused by the other
-// half recomputes this half's strip bit for bit), so a pair's result is the
-// same whichever haplotype shares its warp, or none; the plain schedule runs
-// one pair per item on this kernel and gives the same bits.
+// Every choice above depends on the item's own data (a first pair's boosts on
+// that pair alone, per half; a re-run caused by the other half recomputes this
+// half's strip bit for bit; the later pairs' on the first pair's
+// measurements), and the final log is taken as ln f + (e - E) ln 2 with the
+// sum z = f 2^e, so the bits do not depend on which powers of two the boosts
+// took.  The plain schedule forms the same items and gives the same bits.
 #pragma once
 #include "pairhmm_kernel.cuh"
 
