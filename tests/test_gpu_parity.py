@@ -660,6 +660,36 @@ def test_long_read_kernel_two_haplotypes_per_warp(err, n_haps):
     eng.close()
 
 
+def test_long_reads_against_unrelated_haplotypes():
+    """Reads of 300-2,000 bases against random haplotypes of other lengths (likelihoods thousands of
+    bits below a perfect match, alignment families trading places across rows): the long-read
+    kernel keeps what it holds exactly and hands the rest to the drift and FP64 tiers, every pair
+    within 1e-4 log10 of the FP64 oracle, in items of 2 and of 8 haplotypes."""
+    rng = np.random.default_rng(2718)
+    regions = []
+    for n in (300, 700, 1200, 2000):
+        haps = [S._random_hap(rng, int(m)) for m in rng.integers(150, 2600, 5)]
+        haps[0] = S._random_hap(rng, n + 200)
+        reads = [S._random_hap(rng, n)]
+        # and one read drawn from the first haplotype at 8% substitutions
+        r = haps[0][100:100 + n].copy()
+        for i in np.flatnonzero(rng.random(n) < 0.08):
+            r[i] = S.ALPHABET[S.ALPHABET != r[i]][rng.integers(0, 3)]
+        reads.append(r)
+        quals = [rng.choice(S.Q_LEVELS, n).astype(np.uint8) for _ in reads]
+        regions.append((haps, reads, quals))
+    w = S._assemble("unrelated", regions, S.GAP_Q45, S.EXT_Q10, {})
+    want = _oracle_workload(w)
+    eng = native.Engine(0, 4096)
+    batched, _ = native.make_params(w.gap, w.ext, False, native.VD_PRECISION_MIXED)
+    for group in (2, 8):
+        eng.set_tuning(long_group=group)
+        got, st = eng.forward(_packed(w), batched)
+        assert_mixed_close(got, want)
+        assert st.long_strips > 0
+    eng.close()
+
+
 @pytest.mark.parametrize("mode", ["warp", "block", "single"])
 def test_error_rich_long_read_regions_every_long_path(mode):
     """The mixed-length workload's long-read regions (2-8 reads of 1-10 kb at 6% substitution and
