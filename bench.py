@@ -499,25 +499,9 @@ def main():
         from vardepth_b200 import autotune
         tlog = []
         t0 = time.perf_counter()
-        best = autotune.autotune(engine, mine, params, use_cache=False, log=tlog, stratify=True)
+        best = autotune.autotune(engine, mine, params, use_cache=False, log=tlog, stratify=True, confirm=True)
         chosen = {k: best[k] for k in autotune.DEFAULT}
-        # the sample's choice is confirmed on the whole batch: one captured run of each setting
-        confirm = None
-        if chosen != autotune.DEFAULT:
-            def full_ms(setting):
-                autotune._apply(engine, setting)
-                fp = engine.plan(mine, params)
-                try:
-                    fp.run()
-                    return fp.run().kernel_ms
-                finally:
-                    fp.close()
-            ms_d, ms_c = full_ms(autotune.DEFAULT), full_ms(chosen)
-            kept = chosen if ms_c < ms_d else dict(autotune.DEFAULT)
-            autotune._apply(engine, kept)
-            confirm = {"batch_ms_default": round(ms_d, 3), "batch_ms_chosen": round(ms_c, 3),
-                       "kept": "chosen" if kept is chosen else "default"}
-            chosen = kept
+        confirm = best.get("whole_batch")
         tuned = {"chosen": chosen, "default": autotune.DEFAULT,
                  "samples_regions": best.get("samples"), "sample_ms_default": best.get("default_ms"),
                  "sample_ms_chosen": best.get("sample_ms"), "trials": tlog, "whole_batch": confirm,

@@ -139,11 +139,14 @@ def split_samples(packed: native.Packed, fraction: float = 0.02, min_regions: in
 
 
 def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int = 3, use_cache: bool = True,
-             log: list | None = None, stratify: bool = False) -> dict:
+             log: list | None = None, stratify: bool = False, confirm: bool = False) -> dict:
     """Choose vd_tuning for this batch shape by timing candidates and leave the best on the
     engine.  With stratify=False ``packed`` is already the sample every knob is timed on; with
     stratify=True it is the whole batch (region form) and the long-read knobs are timed on its
-    long-read regions, the others on a sample of its short-read regions (split_samples)."""
+    long-read regions, the others on a sample of its short-read regions (split_samples).
+    With confirm=True a choice other than the default is timed once more against the default
+    on ``packed`` itself and kept only if faster there (``whole_batch`` in the result): a
+    sample cannot show how a persistent kernel's tail behaves on the whole batch."""
     if stratify:
         short_s, long_s = split_samples(packed)
     else:
@@ -180,6 +183,14 @@ def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int 
                 if ms < best_ms * 0.99:
                     best, best_ms = cand, ms
         sample_ms[name] = round(best_ms, 3)
+    whole = None
+    if confirm and {k: best[k] for k in DEFAULT} != DEFAULT:
+        ms_d = _time(engine, packed, params, DEFAULT, 1)
+        ms_c = _time(engine, packed, params, best, 1)
+        whole = {"batch_ms_default": round(ms_d, 3), "batch_ms_chosen": round(ms_c, 3),
+                 "kept": "chosen" if ms_c < ms_d else "default"}
+        if ms_c >= ms_d:
+            best = dict(DEFAULT)
     _apply(engine, best)
     if log is not None:
         log.extend({"sample": nm, "setting": t, "ms": round(ms, 3)} for nm, t, ms in trials)
@@ -190,6 +201,6 @@ def autotune(engine: native.Engine, packed: native.Packed, params, repeats: int 
             CACHE.write_text(json.dumps(cache, indent=1))
         except OSError:
             pass
-    return dict(best, sample_ms=sample_ms, default_ms=default_ms, cached=False,
+    return dict(best, sample_ms=sample_ms, default_ms=default_ms, cached=False, whole_batch=whole,
                 samples={k: (None if v is None else int(len(v.region_read_off) - 1))
                          for k, v in (("short", short_s), ("long", long_s))})
