@@ -219,6 +219,30 @@ def test_drift_boosts_cancel_exactly():
         assert abs(plain - want) <= 1e-9 * abs(want)
 
 
+def test_long_kernel_lane_boosts_cancel_exactly():
+    """The long-read kernel's boosts: lane L scales everything its first row takes from above by
+    2^k_L (folded into that row's hit, miss, K and X), i.e. a per-row boost on every R-th row
+    only, with shares of either sign as a re-run's measured lane decays give them.  The folded
+    recurrence with such boosts equals the unboosted one and the FP64 oracle."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(29)
+    for R in (4, 8):
+        hap = "".join(rng.choice(list("ACGT"), 90))
+        n = 60
+        read = list(hap[10:10 + n])
+        for i in np.flatnonzero(rng.random(n) < 0.08):
+            read[i] = "ACGT"[("ACGT".index(read[i]) + 1) % 4]
+        read = "".join(read)
+        qual = rng.choice([10, 20, 30, 40], n).astype(np.uint8)
+        boost = np.zeros(n, np.int64)
+        boost[::R] = rng.integers(-20, 41, len(boost[::R]))
+        plain = _folded_forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10)
+        lanes = _folded_forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10, boost=boost)
+        want = O.forward(read, qual, hap, S.GAP_Q45, S.EXT_Q10)
+        assert abs(lanes - plain) <= 1e-12 * abs(plain)
+        assert abs(plain - want) <= 1e-9 * abs(want)
+
+
 def _pair_list_mirror(pairs):
     """The regrouping of vd_score_pair_list restated: distinct reads (bases, qualities) and
     haplotypes numbered in order of first appearance; reads asking for the same set of
